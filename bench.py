@@ -1,0 +1,340 @@
+"""Benchmark: grid-point RK-stage updates/s of the plain FP64 channel DNS on B200.
+
+Workload (one GPU): the production grid nP = (256, 192, 193) (x, spanwise,
+wall-normal; 256 x 193 x 192 in the x / wall-normal / spanwise order), i.e.
+9,486,336 points with 9,217,660 updated.  SSP-RK3 with dt from CFL 0.6,
+tanh wall stretching beta = 2.2, Ma 1.5, Re 3000, Pr 0.72, mu ~ T^0.7,
+isothermal walls, periodic x and z, lagged wall-shear forcing with
+statistics every 10 steps.  It starts from the seeded laminar +-10 % start.
+
+One "step" is one full RK3 time step (3 stages).  The metric counts
+interior points x stages per second, summed over all GPUs (replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "grid-point RK-stage updates/s"
+UNIT = "stage-updates/s"
+GRID = (256, 192, 193)
+BETA = 2.2
+CFL = 0.6
+ISTAT = 10
+
+
+def workload(nP=GRID):
+    from compchan3dmpi_b200 import baseline_params, mesh_tanh, laminar_noise, cfl_dt
+    x3, jac, inv = mesh_tanh(nP[2], BETA)
+    p = baseline_params(nP, istat=ISTAT)
+    var = laminar_noise(p, x3, seed=1234)
+    p = p.with_(dt=cfl_dt(var, p, jac, CFL))
+    return p, x3, jac, inv, var
+
+
+def config_dict(p, n_gpus):
+    n1, n2, n3 = p.nP
+    return {
+        "workload": f"plain FP64 DNS {n1}x{n3}x{n2} (x*wall-normal*spanwise), SSP-RK3 CFL {CFL}, "
+                    f"tanh beta {BETA}",
+        "nP": list(p.nP),
+        "points": n1 * n2 * n3,
+        "updated_points": p.n_interior,
+        "stages_per_step": p.stages,
+        "dt": p.dt,
+        "Ma": p.Mac, "Re": p.Re, "Pr": p.Pr,
+        "istat": p.istat,
+        "parallelism": f"replicas x{n_gpus}",
+        "l2_policy": "inputs larger than L2 (state 3 x 400 MB per GPU, L2 126 MB); no flush",
+    }
+
+
+# --------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names[1:], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- peaks
+def hbm_peak():
+    f = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(f) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def measured_traffic(p, n_int):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
+    f = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    try:
+        with open(f) as fh:
+            d = json.load(fh)
+    except (OSError, ValueError):
+        return None
+    bpp = d.get("dram_bytes_per_updated_point_per_stage")
+    if bpp is None:
+        return None
+    return float(bpp) * n_int
+
+
+# --------------------------------------------------------------- CPU
+def cpu_baseline(nP=GRID, budget_s=20.0, threads=None):
+    """The oracle (C restatement, OpenMP) on the host cores: one RK3 stage at
+    a time on a wall-normal slab of the grid, sized to the time budget."""
+    from oracle import oracle as O
+    p, x3, jac, inv, var = workload(nP)
+    O.build()
+    nthreads = threads or os.cpu_count()
+    o = O.Oracle(p, x3, jac, inv, threads=nthreads)
+    o.upload(var)
+    t0 = time.perf_counter()
+    o.stage(1)
+    t1 = time.perf_counter()
+    per_stage = t1 - t0
+    n = max(1, min(3, int(budget_s / max(per_stage, 1e-3))))
+    t0 = time.perf_counter()
+    for it in range(n):
+        o.stage(2 if it % 2 == 0 else 3)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": p.n_interior * n / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n} RK3 stage(s) of the full {nP} grid after 1 untimed stage, "
+                      f"C restatement with OpenMP ({O.num_threads()} threads); not the Fortran binary "
+                      f"(no Fortran compiler on this image)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (the oracle port) on the
+    host cores, same metric/config; rank 0 only."""
+    from compchan3dmpi_b200.replicas import from_env
+    r = from_env()
+    if r.rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    nthreads = os.cpu_count()
+    p, x3, jac, inv, var = workload(GRID)
+    o = O.Oracle(p, x3, jac, inv, threads=nthreads)
+    o.upload(var)
+    # each bench step is one RK3 stage on the full grid; the budget caps the count
+    t0 = time.perf_counter()
+    o.stage(1)
+    per = time.perf_counter() - t0
+    budget = float(os.environ.get("CHAN_REF_BUDGET_S", "150"))
+    K, W = args.steps, args.warmup
+    total = K + W
+    if total * per > budget:
+        scale = budget / (total * per)
+        K = max(3, int(K * scale))
+        W = max(1, min(W, int(W * scale) or 1))
+    for s in range(W):
+        o.stage(2 + s % 2)
+    t0 = time.perf_counter()
+    for s in range(K):
+        o.stage(2 + s % 2)
+    dt = time.perf_counter() - t0
+    o.close()
+    val = p.n_interior * K / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / K * 1e3 * p.stages,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded laminar Poiseuille +-10%)", "config": config_dict(p, 1),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{K} timed RK3 stages (after {W} warm-up) of the full {GRID} grid, "
+                                   "C restatement of the reference with OpenMP; the Fortran reference "
+                                   "cannot be built (no Fortran compiler or MPI on this image)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU
+def run_ours(args):
+    import torch
+    from compchan3dmpi_b200 import Channel
+    from compchan3dmpi_b200 import replicas as R
+
+    ranks = R.init("nccl" if args.gpus > 1 else "gloo")
+    dev = ranks.local_rank
+    torch.cuda.set_device(dev)
+    p, x3, jac, inv, var = workload(tuple(args.grid))
+    p = p.with_(device=dev)
+    n_int = p.n_interior
+    K, W = args.steps, args.warmup
+
+    ch = Channel(p, x3, jac, inv)
+    stream = torch.cuda.ExternalStream(ch.stream_handle(), device=torch.device("cuda", dev))
+
+    # ---------------- device-timed region (inputs resident in HBM)
+    ch.init_sol_v(var)
+    ch.step(W)
+    ch.profile(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(dev)
+    R.barrier(ranks)
+    torch.cuda.synchronize()
+    ch.sync()
+    clocks.start()
+    ev0.record(stream)
+    ch.step_async(K)
+    ev1.record(stream)
+    st = ch.sync()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    R.barrier(ranks)
+    ms = ev0.elapsed_time(ev1)
+    prof_ms, prof_cnt = ch.profile_read()
+    ch.profile(False)
+    ms_max = R.max_over_ranks(ranks, ms)
+    stage_ms = prof_ms[0] / max(int(prof_cnt[0]), 1)
+    stage_ms_max = R.max_over_ranks(ranks, stage_ms)
+
+    # ---------------- end to end through the C ABI with host buffers
+    # the reference's driver loop: restart read (upload), every step a call that
+    # returns its status, statistics read every istat steps, final field write
+    host_in = torch.empty(var.shape, dtype=torch.float64).pin_memory()
+    host_in.numpy()[...] = var
+    host_out = torch.empty(var.shape, dtype=torch.float64).pin_memory()
+    n3 = p.nP[2]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    R.barrier(ranks)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ch.init_sol_v(host_in.numpy())
+    nstats = 0
+    for s in range(1, K + 1):
+        ch.step(1)
+        if s % p.istat == 0:
+            tau, s1, s2, cc = ch.stats()
+            nstats += 1
+    ch.download(out=host_out.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    R.barrier(ranks)
+    e2e_ms = R.max_over_ranks(ranks, e0.elapsed_time(e1))
+    n_pts = p.nP[0] * p.nP[1] * p.nP[2]
+    h2d = 7 * n_pts * 8
+    d2h = 7 * n_pts * 8 + K * 48 + nstats * (23 * n3 + 2) * 8
+
+    status_ok = (st == 0)
+    ch.close()
+
+    if ranks.is_root:
+        stages = p.stages
+        value = ranks.world * n_int * stages * K / (ms_max / 1e3)
+        e2e_val = ranks.world * n_int * stages * K / (e2e_ms / 1e3)
+        bpp = (80 + 120 * (stages - 1)) / stages   # algorithmic bytes per updated point per stage launch
+        achieved = n_int * bpp / (stage_ms_max / 1e3) / 1e9
+        peak, peak_kind = hbm_peak()
+        traffic = measured_traffic(p, n_int)
+        # stage + wall-BC kernels per stage, plus the statistics kernel on its cadence
+        launches = K * 2 * stages + sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded laminar Poiseuille +-10%)",
+            "config": config_dict(p, ranks.world),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_stage<32,8>", "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": n_int * bpp,
+                         "stage_kernel_ms": stage_ms_max,
+                         "stage_share_of_step": prof_ms[0] / max(sum(prof_ms), 1e-12)},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                    "calls": "chan_upload(var) + K x chan_step(1) + chan_stats every istat + chan_download(var)"},
+            "gpu_launches": int(launches),
+            "clocks": ck,
+            "status_ok": status_ok,
+        }
+        if ranks.world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(tuple(args.grid), budget_s=args.cpu_budget)
+        print(json.dumps(line), flush=True)
+    R.finalize(ranks)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

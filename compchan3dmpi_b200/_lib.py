@@ -1,0 +1,96 @@
+"""ctypes binding of ``libchanrhs.so`` (the C ABI in include/chanrhs.h).
+
+The shared library is built in-tree by ``compchan3dmpi_b200.build``.  There
+is no fallback: if the library is missing, loading fails with an error that
+says how to build it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIBDIR = HERE / "lib"
+LIBNAME = "libchanrhs.so"
+
+CHAN_OK, CHAN_BLOWUP, CHAN_NONFINITE = 0, 1, 2
+CHAN_EINVAL, CHAN_ENOMEM, CHAN_ECUDA, CHAN_ESTATE = -1, -2, -3, -4
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I32 = ctypes.POINTER(ctypes.c_int32)
+_I64 = ctypes.POINTER(ctypes.c_int64)
+
+
+class ChanParamsC(ctypes.Structure):
+    """Mirror of ``struct chan_params``."""
+    _fields_ = [
+        ("nP", ctypes.c_int32 * 3),
+        ("istat", ctypes.c_int32),
+        ("rk_scheme", ctypes.c_int32),
+        ("forcing", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("Re", ctypes.c_double),
+        ("Mac", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("Pr", ctypes.c_double),
+        ("gama", ctypes.c_double),
+        ("Pe", ctypes.c_double * 3),
+        ("Lx", ctypes.c_double),
+        ("Ly", ctypes.c_double),
+        ("Tw", ctypes.c_double * 2),
+    ]
+
+
+# every symbol declared in include/chanrhs.h: (name, restype, argtypes)
+SIGNATURES = [
+    ("chan_init", ctypes.c_int, [ctypes.POINTER(ChanParamsC), _D, _D, _D, ctypes.POINTER(ctypes.c_void_p)]),
+    ("chan_upload", ctypes.c_int, [ctypes.c_void_p, _D, ctypes.c_int64, ctypes.c_double]),
+    ("chan_stage", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("chan_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("chan_step_async", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("chan_check", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_tau_wall", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_avg_spatial", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_stats", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D]),
+    ("chan_set_forcing", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D]),
+    ("chan_download", ctypes.c_int, [ctypes.c_void_p, _D]),
+    ("chan_status", ctypes.c_int, [ctypes.c_void_p, _I32, _I64, _D]),
+    ("chan_sync", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("chan_profile_read", ctypes.c_int, [ctypes.c_void_p, _D, _I64]),
+    ("chan_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("chan_device_bytes", ctypes.c_int64, [ctypes.c_void_p]),
+    ("chan_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("chan_version", ctypes.c_char_p, []),
+    ("chan_free", None, [ctypes.c_void_p]),
+]
+
+_lib = None
+
+
+def lib_path() -> Path:
+    return Path(os.environ.get("CHANRHS_LIB", str(LIBDIR / LIBNAME)))
+
+
+def load():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not p.exists():
+        raise RuntimeError(f"{p} not found: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                           "or `python -m compchan3dmpi_b200.build`")
+    L = ctypes.CDLL(str(p))
+    for name, res, args in SIGNATURES:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def dptr(a):
+    return a.ctypes.data_as(_D)

@@ -1,0 +1,205 @@
+"""Host-side mirror of the reference's solver interface.
+
+The reference drives its hot path from a Fortran main program through these
+subroutines (v1.10/codes/main_v1.10.f90:20-53):
+
+    readParam, calcMeshParam, calcCoeffs   -> Channel(params, x3, jac, invJac)
+    readInputFile + initSolV + share2P     -> Channel.init_sol_v(var) / read_input_file(path)
+    calcFlux, calcSolV, share2P, calcPrim,
+    share2P, calcBC (one RK stage)         -> Channel.stage(iter)
+    the time loop                          -> Channel.step(n)
+    checkSoln                              -> Channel.check_soln()
+    calcTauWall                            -> Channel.calc_tau_wall()
+    avgSpatial                             -> Channel.avg_spatial()
+    writeSoln                              -> Channel.write_soln(path)
+
+Every call goes through the C ABI of ``libchanrhs.so``.  Errors are raised
+where the reference would ``stop``: ``BlowUpError`` for rho<0 or T<0
+(v1.9/codes/main_v1.9.f90:709-743), ``ChanError`` for usage/IO/CUDA errors.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import ChanParams
+
+
+class ChanError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"chanrhs error {code}: {msg}")
+        self.code = code
+
+
+class BlowUpError(ChanError):
+    def __init__(self, code, msg, ijk, nstep):
+        super().__init__(code, msg)
+        self.ijk = ijk
+        self.nstep = nstep
+
+
+def to_c_params(p: ChanParams) -> _lib.ChanParamsC:
+    c = _lib.ChanParamsC()
+    c.nP[:] = [int(n) for n in p.nP]
+    c.istat = int(p.istat)
+    c.rk_scheme = int(p.rk_scheme)
+    c.forcing = int(p.forcing)
+    c.device = int(p.device)
+    c.flags = 0
+    c.Re = float(p.Re); c.Mac = float(p.Mac); c.dt = float(p.dt); c.Pr = float(p.Pr); c.gama = float(p.gama)
+    c.Pe[:] = [float(x) for x in p.Pe]
+    c.Lx = float(p.Lx); c.Ly = float(p.Ly)
+    c.Tw[:] = [float(x) for x in p.Tw]
+    return c
+
+
+class Channel:
+    def __init__(self, params: ChanParams, x3, jac, invJac):
+        self.L = _lib.load()
+        self.params = params
+        self.nP = tuple(int(n) for n in params.nP)
+        self.x3 = np.ascontiguousarray(x3, dtype=np.float64)
+        self.jac = np.ascontiguousarray(jac, dtype=np.float64)
+        self.invJac = np.ascontiguousarray(invJac, dtype=np.float64)
+        if self.x3.shape != (self.nP[2],) or self.jac.shape != self.x3.shape or self.invJac.shape != self.x3.shape:
+            raise ValueError("x3, jac, invJac must have nP3 entries")
+        self._cp = to_c_params(params)
+        h = ctypes.c_void_p()
+        r = self.L.chan_init(ctypes.byref(self._cp), _lib.dptr(self.x3), _lib.dptr(self.jac),
+                             _lib.dptr(self.invJac), ctypes.byref(h))
+        if r != 0:
+            raise ChanError(r, self.L.chan_last_error(None).decode())
+        self._h = h
+
+    # -------------------------------------------------------------- plumbing
+    def _check(self, r):
+        if r == 0:
+            return 0
+        if r == _lib.CHAN_BLOWUP:
+            ijk, n, _ = self.status_detail()
+            raise BlowUpError(r, f"blow-up (rho<0 or T<0) at i,j,k={ijk} in step {n}", ijk, n)
+        if r == _lib.CHAN_NONFINITE:
+            return r
+        raise ChanError(r, self.L.chan_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.chan_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        n1, n2, n3 = self.nP
+        return (7, n3, n2, n1)
+
+    # ------------------------------------------------------ reference names
+    def init_sol_v(self, var: np.ndarray, nstep: int = 0, time: float = 0.0):
+        v = np.ascontiguousarray(var, dtype=np.float64)
+        if v.shape != self.shape:
+            raise ValueError(f"var must have shape {self.shape}")
+        self._check(self.L.chan_upload(self._h, _lib.dptr(v), int(nstep), float(time)))
+
+    def read_input_file(self, path):
+        from .deck import read_3d_dat
+        var, time, nstep, *_ = read_3d_dat(path, self.nP)
+        self.init_sol_v(var, nstep, time)
+        return var
+
+    def stage(self, it: int):
+        return self._check(self.L.chan_stage(self._h, int(it)))
+
+    def step(self, n: int = 1):
+        return self._check(self.L.chan_step(self._h, int(n)))
+
+    def step_async(self, n: int = 1):
+        return self._check(self.L.chan_step_async(self._h, int(n)))
+
+    def sync(self):
+        return self._check(self.L.chan_sync(self._h))
+
+    def check_soln(self):
+        return self._check(self.L.chan_check(self._h))
+
+    def calc_tau_wall(self):
+        return self._check(self.L.chan_tau_wall(self._h))
+
+    def avg_spatial(self):
+        return self._check(self.L.chan_avg_spatial(self._h))
+
+    def stats(self):
+        n3 = self.nP[2]
+        tau = np.zeros(2); s1 = np.zeros((7, n3)); s2 = np.zeros((7, n3)); c = np.zeros((9, n3))
+        self._check(self.L.chan_stats(self._h, _lib.dptr(tau), _lib.dptr(s1), _lib.dptr(s2), _lib.dptr(c)))
+        return tau, s1, s2, c
+
+    def set_forcing(self, tauL: float, tauU: float, rhobar):
+        rb = np.ascontiguousarray(rhobar, dtype=np.float64)
+        self._check(self.L.chan_set_forcing(self._h, float(tauL), float(tauU), _lib.dptr(rb)))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape)
+        assert out.shape == self.shape and out.dtype == np.float64 and out.flags.c_contiguous
+        self._check(self.L.chan_download(self._h, _lib.dptr(out)))
+        return out
+
+    def write_soln(self, path):
+        from .deck import write_3d_dat
+        from .mesh import periodic_coords
+        var = self.download()
+        _, n, t = self.status_detail()
+        write_3d_dat(path, var, periodic_coords(self.nP[0], self.params.Lx),
+                     periodic_coords(self.nP[1], self.params.Ly), self.x3, t, n)
+
+    def status_detail(self):
+        ijk = (ctypes.c_int32 * 3)()
+        n = ctypes.c_int64()
+        t = ctypes.c_double()
+        self.L.chan_status(self._h, ijk, ctypes.byref(n), ctypes.byref(t))
+        return tuple(ijk), n.value, t.value
+
+    def status(self) -> int:
+        ijk = (ctypes.c_int32 * 3)()
+        return self.L.chan_status(self._h, ijk, None, None)
+
+    @property
+    def nstep(self):
+        return self.status_detail()[1]
+
+    @property
+    def time(self):
+        return self.status_detail()[2]
+
+    # -------------------------------------------------------- measurement
+    def profile(self, enable: bool):
+        self._check(self.L.chan_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        ms = np.zeros(3)
+        cnt = np.zeros(3, dtype=np.int64)
+        self._check(self.L.chan_profile_read(self._h, _lib.dptr(ms), cnt.ctypes.data_as(_lib._I64)))
+        return ms, cnt
+
+    def stream_handle(self) -> int:
+        return int(self.L.chan_stream(self._h) or 0)
+
+    def device_bytes(self) -> int:
+        return int(self.L.chan_device_bytes(self._h))
+
+
+def version() -> str:
+    return _lib.load().chan_version().decode()

@@ -1,0 +1,874 @@
+// chan_kernels.cuh -- sm_100a kernels of the compressible-channel time step.
+//
+// Device layout (all FP64):
+//   Q  [5][nP3+2][nP2+2][px]   conservative state rho,rho*u,rho*v,rho*w,rho*E.
+//                              Indices equal the reference's solV(0:nP1+1,
+//                              0:nP2+1,0:nP3+1,1:5) (v1.10/codes/main_v1.9.f90:43).
+//                              The 2-deep periodic ghosts are written by the
+//                              stage kernel itself, so every read is plain.
+//   WP [2][8][nP2+2][px]       primitive state of the two wall planes k=1, k=nP3:
+//                              rho,u,v,w,E,T,p,mu.  The wall pressure is a
+//                              state variable of its own (pressure BC).
+//   CS [nP3+2][4][7]           var at the four periodic corner columns.  The
+//                              reference never refreshes these (its halo
+//                              datatypes skip corners), yet its plane
+//                              statistics sum them; kept only for that.
+//
+// One RK stage = k_stage (fluxes + update, fused) + k_wall (wall BC +
+// pressure BC).  k_stats runs every istat steps.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chan {
+
+struct DevStatus {
+    int blown;             // rho<0 or T<0 seen (reference blow-up test)
+    int ijk[3];            // one offending point, 1-based reference indices
+    int nonfinite;         // NaN/Inf seen
+    int nf_ijk[3];
+    long long blown_step;  // step in which the blow-up happened
+    long long pad;
+};
+
+struct KParams {
+    // geometry
+    int n1, n2, n3, px, NJ, kchunk;
+    long long plane, vol;
+    // state
+    const double *qin, *qbase;
+    double *qout;
+    double *wp;
+    const double *cs;
+    // per-k tables [nP3+2]
+    const double *czh;    // 0.5*invdXi*invJac(k)
+    const double *cz8;    // invdXi*invJac(k)/8
+    const double *cz12;   // invdXi*invJac(k)/12
+    const double *pez;    // Re*dXi*jac(k)
+    // forcing / stats
+    double *stat;         // stat1[7*n3] | stat2[7*n3] | corr[9*n3] | tau[2]
+    DevStatus *status;
+    // physics
+    double invRe, ggM, ggMh, gM2, inv_gM2, kq, two3rd;
+    double hdx, hdy, sx8, sx12, sy8, sy12, invdx, invdy;
+    double pex, pey, pez_val;   // Re*dx, Re*dy (x,y Peclet prefactors); PezVal
+    double PexVal, PeyVal;
+    double inv_dz1, inv_dzN;
+    double Twb, Twt, muwb, muwt;
+    double f1[3], f2[3], b1[3], b2[3];  // wall one-sided coefficients
+    // RK stage
+    double rk_a, rk_b, rk_cdt;
+    int rk_mode;          // 0: in + cdt*R ; 1: base + cdt*R ; 2: a*base + b*in + cdt*R
+    int check;            // last stage of a step: run the blow-up test
+    int force_on;
+    long long step;       // step number being computed
+};
+
+__device__ __forceinline__ bool frozen(const DevStatus *st, long long step)
+{
+    // after a blow-up the reference stops; later steps do nothing here
+    volatile const DevStatus *v = st;
+    return v->blown && v->blown_step < step;
+}
+
+__device__ __forceinline__ void flag_blown(DevStatus *st, int i, int j, int k, long long step)
+{
+    if (atomicCAS(&st->blown, 0, 1) == 0) {
+        st->ijk[0] = i; st->ijk[1] = j; st->ijk[2] = k;
+        st->blown_step = step;
+    }
+}
+
+__device__ __forceinline__ void flag_nonfinite(DevStatus *st, int i, int j, int k)
+{
+    if (atomicCAS(&st->nonfinite, 0, 1) == 0) {
+        st->nf_ijk[0] = i; st->nf_ijk[1] = j; st->nf_ijk[2] = k;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inviscid stencil weights.  Both branches of the reference's hybrid scheme are
+// linear in the conservative variable once the velocities are fixed, so a
+// point's flux derivative along one axis is sum_m w[m]*Q(offset m-2) with
+// weights shared by all five variables.
+//  central : (-u2 Q2 + 8 u1 Q1 - 8 u-1 Q-1 + u-2 Q-2) /(12 d)   main_v1.9.f90:364-368
+//  QUICK   : ue*Qe - uw*Qw, face values upwinded on the face velocity sign,
+//            the four sign branches of main_v1.9.f90:335-361
+__device__ __forceinline__ void inv_weights(double um2, double um1, double u0, double up1, double up2,
+                                            bool quick, double s8, double s12, double w[5])
+{
+    if (quick) {
+        const double r1 = (u0 + up1) * 0.5;  // tmpR1, east face
+        const double r2 = (u0 + um1) * 0.5;  // tmpR2, west face
+        const bool e = r1 >= 0.0, f = r2 >= 0.0;
+        const double R1 = r1 * s8, R2 = r2 * s8;
+        // east face value at offsets -1,0,+1,+2 ; west face at -2,-1,0,+1
+        const double ae_m1 = e ? -1.0 : 0.0, ae_0 = e ? 6.0 : 3.0, ae_1 = e ? 3.0 : 6.0, ae_2 = e ? 0.0 : -1.0;
+        const double bw_m2 = f ? -1.0 : 0.0, bw_m1 = f ? 6.0 : 3.0, bw_0 = f ? 3.0 : 6.0, bw_1 = f ? 0.0 : -1.0;
+        w[0] = -R2 * bw_m2;
+        w[1] = R1 * ae_m1 - R2 * bw_m1;
+        w[2] = R1 * ae_0 - R2 * bw_0;
+        w[3] = R1 * ae_1 - R2 * bw_1;
+        w[4] = R1 * ae_2;
+    } else {
+        w[0] = um2 * s12;
+        w[1] = -8.0 * um1 * s12;
+        w[2] = 0.0;
+        w[3] = 8.0 * up1 * s12;
+        w[4] = -(up2 * s12);
+    }
+}
+
+__device__ __forceinline__ double wsum(const double w[5], double q0, double q1, double q2, double q3, double q4)
+{
+    return (((w[0] * q0 + w[1] * q1) + w[2] * q2) + w[3] * q3) + w[4] * q4;
+}
+
+// ---------------------------------------------------------------------------
+// Viscous / pressure flux vectors of main_v1.9.f90:457-538 in stress form.
+// fD2..fD5 (fD1 = 0).  The energy component uses the identity
+//   ggM*u*p + dissF = ggM*(u*fD2 + v*fD3 + w*fD4),
+// which is the reference's dissF regrouped (same terms, different rounding).
+struct Slot {
+    const double *U, *V, *W, *T;
+};
+
+template <int BX>
+__device__ __forceinline__ void visc_fx(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
+                                        const double *MU, const double *PR, int b, double czt, double f[4])
+{
+    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
+    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
+    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
+    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
+    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
+    const double Tx = (s.T[b + 1] - s.T[b - 1]) * P.hdx;
+    const double uz = (sp.U[b] - sm.U[b]) * czt;
+    const double wz = (sp.W[b] - sm.W[b]) * czt;
+    const double mu = MU[b], pr = PR[b];
+    const double mr = mu * P.invRe;
+    const double div = (ux + vy) + wz;
+    const double f2 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * ux;
+    const double f3 = -(mr * (vx + uy));
+    const double f4 = -(mr * (wx + uz));
+    f[0] = f2;
+    f[1] = f3;
+    f[2] = f4;
+    f[3] = -((P.kq * mu) * Tx) + P.ggM * ((s.U[b] * f2 + s.V[b] * f3) + s.W[b] * f4);
+}
+
+template <int BX>
+__device__ __forceinline__ void visc_fy(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
+                                        const double *MU, const double *PR, int b, double czt, double g[4])
+{
+    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
+    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
+    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
+    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
+    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
+    const double Ty = (s.T[b + BX] - s.T[b - BX]) * P.hdy;
+    const double vz = (sp.V[b] - sm.V[b]) * czt;
+    const double wz = (sp.W[b] - sm.W[b]) * czt;
+    const double mu = MU[b], pr = PR[b];
+    const double mr = mu * P.invRe;
+    const double div = (ux + vy) + wz;
+    const double g2 = -(mr * (vx + uy));
+    const double g3 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * vy;
+    const double g4 = -(mr * (wy + vz));
+    g[0] = g2;
+    g[1] = g3;
+    g[2] = g4;
+    g[3] = -((P.kq * mu) * Ty) + P.ggM * ((s.U[b] * g2 + s.V[b] * g3) + s.W[b] * g4);
+}
+
+// hD at the thread's own column; z-derivatives supplied by the caller
+template <int BX>
+__device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double mu, double pr, int b,
+                                        double uz, double vz, double wz, double Tz, double h[4])
+{
+    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
+    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
+    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
+    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
+    const double mr = mu * P.invRe;
+    const double div = (ux + vy) + wz;
+    const double h2 = -(mr * (wx + uz));
+    const double h3 = -(mr * (wy + vz));
+    const double h4 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * wz;
+    h[0] = h2;
+    h[1] = h3;
+    h[2] = h4;
+    h[3] = -((P.kq * mu) * Tz) + P.ggM * ((s.U[b] * h2 + s.V[b] * h3) + s.W[b] * h4);
+}
+
+// primitives of one point from the conservative state (calcPrim, main_v1.9.f90:600-609)
+__device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5], double &u, double &v,
+                                             double &w, double &T)
+{
+    const double r = __drcp_rn(q[0]);
+    u = q[1] * r;
+    v = q[2] * r;
+    w = q[3] * r;
+    const double E = q[4] * r;
+    T = E - P.ggMh * ((u * u + v * v) + w * w);
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel.
+//
+// A CTA owns a TI x TJ tile of interior (i,j) columns and marches a chunk of
+// interior planes k = kb..ke.  Shared memory holds, for the tile plus a
+// 2-point halo box ((TI+4) x (TJ+4)):
+//   prims u,v,w,T   of planes t-1, t, t+1   (3-slot ring)
+//   mu, p           of planes t, t+1        (2-slot ring)
+//   Q (5 vars)      of planes t, t+1        (2-slot ring)
+//   fD, gD          of plane t on the tile plus a 1-point halo
+// Each thread keeps its own column's Q and w at t-2, t-1, t+2 and hD at
+// t-1, t, t+1 in registers.  Per output plane the CTA loads one new plane,
+// so Q is read from DRAM once per stage (halo re-reads come from L2).
+template <int TI, int TJ>
+struct StageShape {
+    static constexpr int BX = TI + 4, BY = TJ + 4, NB = BX * BY, NT = TI * TJ;
+    static constexpr int NFX = TJ * (TI + 2), NGY = (TJ + 2) * TI;
+    static constexpr int doubles = 12 * NB + 4 * NB + 10 * NB + 4 * NFX + 4 * NGY;
+    static constexpr size_t bytes = sizeof(double) * (size_t)doubles;
+};
+
+template <int TI, int TJ>
+__global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
+{
+    using S = StageShape<TI, TJ>;
+    constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT;
+    extern __shared__ double smem[];
+    double *sPr = smem;            // [3][4][NB]
+    double *sMP = sPr + 12 * NB;   // [2][2][NB]   mu, p
+    double *sQ = sMP + 4 * NB;     // [2][5][NB]
+    double *sF = sQ + 10 * NB;     // [4][TJ][TI+2]
+    double *sG = sF + 4 * S::NFX;  // [4][TJ+2][TI]
+    __shared__ int s_frozen;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
+    if (tid == 0) s_frozen = frozen(P.status, P.step) ? 1 : 0;
+    __syncthreads();
+    if (s_frozen) return;
+
+    const int i0 = 2 + blockIdx.x * TI, j0 = 2 + blockIdx.y * TJ;
+    const int kb = 2 + blockIdx.z * P.kchunk;
+    const int ke = min(kb + P.kchunk - 1, P.n3 - 1);
+    if (kb > ke) return;
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool col_ok = (i <= n1) && (j <= n2);
+    const bool out_ok = (i <= n1 - 1) && (j <= n2 - 1);
+    const int bc = (ty + 2) * BX + (tx + 2);
+    const long long vol = P.vol, plane = P.plane;
+    const long long colo = (long long)j * P.px + i;
+
+    auto slot = [&](int m) -> Slot {
+        const int s = m % 3;
+        return Slot{sPr + (s * 4 + 0) * NB, sPr + (s * 4 + 1) * NB, sPr + (s * 4 + 2) * NB, sPr + (s * 4 + 3) * NB};
+    };
+    auto smu = [&](int m) { return sMP + ((m & 1) * 2 + 0) * NB; };
+    auto spr = [&](int m) { return sMP + ((m & 1) * 2 + 1) * NB; };
+    auto sq = [&](int m, int v) { return sQ + ((m & 1) * 5 + v) * NB; };
+
+    // fill the ring slots of plane m over the whole box
+    auto load_plane = [&](int m) {
+        const Slot s = slot(m);
+        double *MU = smu(m), *PR = spr(m);
+        const bool wall = (m == 1 || m == n3);
+        const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
+        for (int p = tid; p < NB; p += NT) {
+            const int bj = p / BX, bi = p - bj * BX;
+            const int gi = i0 - 2 + bi, gj = j0 - 2 + bj;
+            if (gi > n1 + 1 || gj > n2 + 1) continue;
+            const long long off = (long long)m * plane + (long long)gj * P.px + gi;
+            double q[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                q[v] = __ldg(P.qin + v * vol + off);
+                sq(m, v)[p] = q[v];
+            }
+            double u, vv, w, T, mu, pr;
+            if (wall) {
+                const long long wo = (long long)gj * P.px + gi;
+                u = W[1 * plane + wo];
+                vv = W[2 * plane + wo];
+                w = W[3 * plane + wo];
+                T = W[5 * plane + wo];
+                pr = W[6 * plane + wo];
+                mu = W[7 * plane + wo];
+            } else {
+                prims_from_q(P, q, u, vv, w, T);
+                pr = (q[0] * T) * P.inv_gM2;
+                const bool r1 = (bi >= 1 && bi <= BX - 2 && bj >= 2 && bj <= BY - 3) ||
+                                (bi >= 2 && bi <= BX - 3 && bj >= 1 && bj <= BY - 2);
+                mu = r1 ? pow(T, 0.7) : 0.0;
+            }
+            ((double *)s.U)[p] = u;
+            ((double *)s.V)[p] = vv;
+            ((double *)s.W)[p] = w;
+            ((double *)s.T)[p] = T;
+            MU[p] = mu;
+            PR[p] = pr;
+        }
+    };
+
+    // own-column Q and u,v,w,T of plane m read straight from memory
+    auto center = [&](int m, double q[5], double &u, double &v, double &w, double &T) {
+        const long long off = (long long)m * plane + colo;
+#pragma unroll
+        for (int c = 0; c < 5; c++) q[c] = __ldg(P.qin + c * vol + off);
+        if (m == 1 || m == n3) {
+            const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane + colo;
+            u = W[1 * plane]; v = W[2 * plane]; w = W[3 * plane]; T = W[5 * plane];
+        } else {
+            prims_from_q(P, q, u, v, w, T);
+        }
+    };
+
+    // hD at the own column of plane m (in ring); dz from (m-1, m+1) values
+    auto hflux = [&](int m, double um, double vm, double wm, double Tm, double up, double vp, double wp_,
+                     double Tp, double h[4]) {
+        const Slot s = slot(m);
+        double sc;
+        if (m == 1) {
+            // one-sided at the bottom wall: (q(2)-q(1))/dz1 ; "m-1" slot is the wall itself
+            sc = P.inv_dz1;
+        } else if (m == n3) {
+            sc = P.inv_dzN;
+        } else {
+            sc = P.czh[m];
+        }
+        visc_fz<BX>(P, s, smu(m)[bc], spr(m)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
+                    (Tp - Tm) * sc, h);
+    };
+
+    // ---------------- prologue: planes kb-1 and kb, hD(kb-1), hD(kb)
+    double qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
+    double wm2 = 0.0;
+    load_plane(kb - 1);
+    load_plane(kb);
+    __syncthreads();
+    {
+        const Slot sA = slot(kb - 1), sB = slot(kb);
+        if (col_ok) {
+            // hD(kb-1)
+            if (kb - 1 == 1) {
+                hflux(1, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+            } else {
+                double q[5], u, v, w, T;
+                center(kb - 2, q, u, v, w, T);
+                hflux(kb - 1, u, v, w, T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+            }
+            // hD(kb)
+            {
+                double q[5], u, v, w, T;
+                center(kb + 1, q, u, v, w, T);
+                hflux(kb, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], u, v, w, T, h0);
+            }
+            if (kb - 2 >= 1) {
+                double u, v, w, T;
+                center(kb - 2, qm2, u, v, w, T);
+                wm2 = w;
+            }
+#pragma unroll
+            for (int c = 0; c < 5; c++) qm1[c] = sq(kb - 1, c)[bc];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 5; c++) qm1[c] = 0.0;
+        }
+    }
+    __syncthreads();
+
+    for (int t = kb; t <= ke; t++) {
+        // ---------- A: plane t+1 into the ring; own column of t+2
+        load_plane(t + 1);
+        double qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
+        if (col_ok && t + 2 <= n3) center(t + 2, qp2, up2, vp2, wp2, Tp2);
+        __syncthreads();
+
+        // ---------- C: viscous flux vectors
+        const Slot s0 = slot(t), sm = slot(t - 1), sp = slot(t + 1);
+        double hp1[4] = {0, 0, 0, 0};
+        if (col_ok) {
+            if (t + 1 == n3)
+                hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], sp.U[bc], sp.V[bc], sp.W[bc], sp.T[bc], hp1);
+            else
+                hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+            const double czt = P.czh[t];
+            const double *MU = smu(t), *PR = spr(t);
+            double f[4];
+            visc_fx<BX>(P, s0, sm, sp, MU, PR, bc, czt, f);
+#pragma unroll
+            for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
+            if (tx == 0) {
+                visc_fx<BX>(P, s0, sm, sp, MU, PR, bc - 1, czt, f);
+#pragma unroll
+                for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + 0] = f[c];
+            }
+            if (tx == TI - 1 && i + 1 <= n1) {
+                visc_fx<BX>(P, s0, sm, sp, MU, PR, bc + 1, czt, f);
+#pragma unroll
+                for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + TI + 1] = f[c];
+            }
+            visc_fy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f);
+#pragma unroll
+            for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + ty + 1) * TI + tx] = f[c];
+            if (ty == 0) {
+                visc_fy<BX>(P, s0, sm, sp, MU, PR, bc - BX, czt, f);
+#pragma unroll
+                for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + 0) * TI + tx] = f[c];
+            }
+            if (ty == TJ - 1 && j + 1 <= n2) {
+                visc_fy<BX>(P, s0, sm, sp, MU, PR, bc + BX, czt, f);
+#pragma unroll
+                for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + TJ + 1) * TI + tx] = f[c];
+            }
+        }
+        __syncthreads();
+
+        // ---------- E: fluxes, source, RK update
+        double q0[5];
+#pragma unroll
+        for (int c = 0; c < 5; c++) q0[c] = sq(t, c)[bc];
+        const double wm1 = sm.W[bc];
+        if (out_ok) {
+            double R[5];
+            const double mu0 = smu(t)[bc];
+            // x
+            {
+                const double *U = s0.U;
+                const bool qk = (P.pex * fabs(q0[1])) > P.PexVal * mu0;
+                double w[5];
+                inv_weights(U[bc - 2], U[bc - 1], U[bc], U[bc + 1], U[bc + 2], qk, P.sx8, P.sx12, w);
+                double F1[5];
+#pragma unroll
+                for (int c = 0; c < 5; c++) {
+                    const double *Q = sq(t, c);
+                    F1[c] = wsum(w, Q[bc - 2], Q[bc - 1], Q[bc], Q[bc + 1], Q[bc + 2]);
+                }
+                R[0] = F1[0];  // F2 of continuity is zero
+#pragma unroll
+                for (int c = 1; c < 5; c++) {
+                    const int r = (c - 1) * TJ + ty;
+                    const double F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * P.hdx;
+                    R[c] = F1[c] + F2;
+                }
+            }
+            // y
+            {
+                const double *V = s0.V;
+                const bool qk = (P.pey * fabs(q0[2])) > P.PeyVal * mu0;
+                double w[5];
+                inv_weights(V[bc - 2 * BX], V[bc - BX], V[bc], V[bc + BX], V[bc + 2 * BX], qk, P.sy8, P.sy12, w);
+                double G1[5];
+#pragma unroll
+                for (int c = 0; c < 5; c++) {
+                    const double *Q = sq(t, c);
+                    G1[c] = wsum(w, Q[bc - 2 * BX], Q[bc - BX], Q[bc], Q[bc + BX], Q[bc + 2 * BX]);
+                }
+                R[0] = R[0] + G1[0];
+#pragma unroll
+                for (int c = 1; c < 5; c++) {
+                    const double G2 = (sG[((c - 1) * (TJ + 2) + ty + 2) * TI + tx] -
+                                       sG[((c - 1) * (TJ + 2) + ty) * TI + tx]) * P.hdy;
+                    R[c] = (R[c] + G1[c]) + G2;
+                }
+            }
+            // z
+            {
+                const double w0 = s0.W[bc], wp1 = sp.W[bc];
+                double w[5];
+                if (t < 3 || t > n3 - 2) {
+                    const double c2 = P.czh[t];
+                    w[0] = 0.0; w[1] = -(wm1 * c2); w[2] = 0.0; w[3] = wp1 * c2; w[4] = 0.0;
+                } else {
+                    const bool qk = (P.pez[t] * fabs(q0[3])) > P.pez_val * mu0;
+                    inv_weights(wm2, wm1, w0, wp1, wp2, qk, P.cz8[t], P.cz12[t], w);
+                }
+                const double czt = P.czh[t];
+                R[0] = R[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(t + 1, 0)[bc], qp2[0]);
+#pragma unroll
+                for (int c = 1; c < 5; c++) {
+                    const double H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(t + 1, c)[bc], qp2[c]);
+                    const double H2 = (hp1[c - 1] - hm1[c - 1]) * czt;
+                    R[c] = (R[c] + H1) + H2;
+                }
+            }
+            // source: lagged wall-shear forcing (main_v1.9.f90:565-571)
+            double src2 = 0.0, src5 = 0.0;
+            if (P.force_on) {
+                const double tau = P.stat[23 * n3 + 0] - P.stat[23 * n3 + 1];
+                const double rb = P.stat[t - 1];
+                src2 = (0.5 * tau) * rb;
+                src5 = (((P.ggM * s0.U[bc]) * 0.5) * tau) * rb;
+            }
+            R[0] = -R[0];
+            R[1] = src2 - R[1];
+            R[2] = -R[2];
+            R[3] = -R[3];
+            R[4] = src5 - R[4];
+            // RK update
+            double qn[5];
+            const long long off = (long long)t * plane + colo;
+            if (P.rk_mode == 0) {
+#pragma unroll
+                for (int c = 0; c < 5; c++) qn[c] = q0[c] + P.rk_cdt * R[c];
+            } else if (P.rk_mode == 1) {
+#pragma unroll
+                for (int c = 0; c < 5; c++) qn[c] = __ldg(P.qbase + c * vol + off) + P.rk_cdt * R[c];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 5; c++)
+                    qn[c] = (P.rk_a * __ldg(P.qbase + c * vol + off) + P.rk_b * q0[c]) + P.rk_cdt * R[c];
+            }
+            // store + periodic images (the ghosts the reference's halo exchange fills)
+            const int im = (i <= 3) ? i + (n1 - 2) : ((i >= n1 - 2) ? i - (n1 - 2) : -1);
+            const int jm = (j <= 3) ? j + (n2 - 2) : ((j >= n2 - 2) ? j - (n2 - 2) : -1);
+            const long long pk = (long long)t * plane;
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                double *O = P.qout + c * vol + pk;
+                O[(long long)j * P.px + i] = qn[c];
+                if (im >= 0) O[(long long)j * P.px + im] = qn[c];
+                if (jm >= 0) O[(long long)jm * P.px + i] = qn[c];
+                if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = qn[c];
+            }
+            if (P.check) {
+                const double tr = qn[0] * qn[4] - P.ggMh * ((qn[1] * qn[1] + qn[2] * qn[2]) + qn[3] * qn[3]);
+                if (qn[0] < 0.0 || (qn[0] > 0.0 && tr < 0.0)) flag_blown(P.status, i, j, t, P.step);
+                bool fin = true;
+#pragma unroll
+                for (int c = 0; c < 5; c++) fin = fin && isfinite(qn[c]);
+                if (!fin) flag_nonfinite(P.status, i, j, t);
+            }
+        }
+        // ---------- F: rotate the column registers
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+            qm2[c] = qm1[c];
+            qm1[c] = q0[c];
+        }
+        wm2 = wm1;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            hm1[c] = h0[c];
+            h0[c] = hp1[c];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Wall BC + pressure BC (main_v1.9.f90:623-720 on the two wall planes).
+// One thread per (i,j) of a wall plane, ghosts included.
+__global__ void k_wall(const KParams P)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int wall = blockIdx.z;
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    if (i > n1 + 1 || j > n2 + 1) return;
+    if (frozen(P.status, P.step)) return;
+    const long long plane = P.plane, vol = P.vol;
+    double *W = P.wp + (size_t)wall * 8 * plane;
+    const long long idx = (long long)j * P.px + i;
+    const double Tw = wall == 0 ? P.Twb : P.Twt;
+    const double pold = W[6 * plane + idx];
+    const double rho = (P.gM2 * pold) / Tw;   // gama*Mac**2*p/T with the previous p
+    double pnew = pold;
+    if (i >= 2 && i <= n1 - 1 && j >= 2 && j <= n2 - 1) {
+        // neighbours at the two planes next to the wall: k2 (adjacent) and k3
+        const int k2 = wall == 0 ? 2 : n3 - 1, k3 = wall == 0 ? 3 : n3 - 2;
+        const double *c1 = wall == 0 ? P.f1 : P.b1;
+        const double *c2 = wall == 0 ? P.f2 : P.b2;
+        // primitive + mu of one interior point, as calcPrim/calcBC produce them
+        auto prim = [&](int ii, int jj, int kk, double &r, double &u, double &v, double &w, double &T,
+                        double &p, double &mu) {
+            const long long o = (long long)kk * plane + (long long)jj * P.px + ii;
+            const double q0 = P.qout[o], q1 = P.qout[vol + o], q2 = P.qout[2 * vol + o];
+            const double q3 = P.qout[3 * vol + o], q4 = P.qout[4 * vol + o];
+            r = q0;
+            u = q1 / q0; v = q2 / q0; w = q3 / q0;
+            const double E = q4 / q0;
+            T = E - P.ggMh * ((u * u + v * v) + w * w);
+            p = (r * T) / P.gM2;
+            mu = pow(T, 0.7);
+        };
+        double r, u, v, w, T, p, mu;
+        double a2, a3, b2, b3;
+        // d/dx of mu*du/dz
+        prim(i + 1, j, k2, r, u, v, w, T, p, mu); a2 = c1[1] * mu * u;
+        prim(i + 1, j, k3, r, u, v, w, T, p, mu); a3 = c1[2] * mu * u;
+        prim(i - 1, j, k2, r, u, v, w, T, p, mu); b2 = c1[1] * mu * u;
+        prim(i - 1, j, k3, r, u, v, w, T, p, mu); b3 = c1[2] * mu * u;
+        const double dudxdz = ((a2 + a3) - (b2 + b3)) * P.hdx;
+        prim(i, j + 1, k2, r, u, v, w, T, p, mu); a2 = c1[1] * mu * v;
+        prim(i, j + 1, k3, r, u, v, w, T, p, mu); a3 = c1[2] * mu * v;
+        prim(i, j - 1, k2, r, u, v, w, T, p, mu); b2 = c1[1] * mu * v;
+        prim(i, j - 1, k3, r, u, v, w, T, p, mu); b3 = c1[2] * mu * v;
+        const double dvdydz = ((a2 + a3) - (b2 + b3)) * P.hdy;
+        double p2, p3, d2, d3, e2, e3;
+        prim(i, j, k2, r, u, v, w, T, p, mu);
+        d2 = c2[1] * mu * w; e2 = c1[1] * r * (w * w); p2 = p;
+        prim(i, j, k3, r, u, v, w, T, p, mu);
+        d3 = c2[2] * mu * w; e3 = c1[2] * r * (w * w); p3 = p;
+        // the wall-point terms vanish: u=v=w=0 there after the wall BC
+        const double d2wdz2 = d2 + d3;
+        const double drhow2dz = e2 + e3;
+        const double lhs = P.invRe * ((-dudxdz - dvdydz) + P.two3rd * ((dudxdz + dvdydz) - 2.0 * d2wdz2)) + drhow2dz;
+        pnew = -((lhs + c1[1] * p2) + c1[2] * p3) / c1[0];
+    }
+    W[0 * plane + idx] = rho;
+    W[1 * plane + idx] = 0.0;
+    W[2 * plane + idx] = 0.0;
+    W[3 * plane + idx] = 0.0;
+    W[4 * plane + idx] = Tw;
+    W[5 * plane + idx] = Tw;
+    W[6 * plane + idx] = pnew;
+    W[7 * plane + idx] = wall == 0 ? P.muwb : P.muwt;
+    if (P.check && i >= 1 && i <= n1 && j >= 1 && j <= n2) {
+        if (rho < 0.0 || Tw < 0.0) flag_blown(P.status, i, j, wall == 0 ? 1 : n3, P.step);
+        if (!isfinite(rho) || !isfinite(pnew)) flag_nonfinite(P.status, i, j, wall == 0 ? 1 : n3);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// var(i,j,k,1:7) as the reference holds it after a stage (used by the
+// statistics, the blow-up scan and downloads).
+__device__ __forceinline__ void ref_var(const KParams &P, const double *q, int i, int j, int k, double x[7])
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    if (k == 1 || k == n3) {
+        const double *W = P.wp + (size_t)(k == 1 ? 0 : 8) * P.plane + (long long)j * P.px + i;
+        x[0] = W[0]; x[1] = W[P.plane]; x[2] = W[2 * P.plane]; x[3] = W[3 * P.plane];
+        x[4] = W[4 * P.plane]; x[5] = W[5 * P.plane]; x[6] = W[6 * P.plane];
+        return;
+    }
+    const bool ci = (i == 1 || i == n1), cj = (j == 1 || j == n2);
+    if (ci && cj) {
+        const int c = (i == 1 ? 0 : 1) + (j == 1 ? 0 : 2);
+        const double *C = P.cs + ((size_t)k * 4 + c) * 7;
+#pragma unroll
+        for (int m = 0; m < 7; m++) x[m] = C[m];
+        return;
+    }
+    const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+    const double q0 = q[o];
+    x[0] = q0;
+    x[1] = q[P.vol + o] / q0;
+    x[2] = q[2 * P.vol + o] / q0;
+    x[3] = q[3 * P.vol + o] / q0;
+    x[4] = q[4 * P.vol + o] / q0;
+    x[5] = x[4] - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
+    x[6] = (x[0] * x[5]) / P.gM2;
+}
+
+// Plane moments (avgSpatial, main_v1.9.f90:995-1025) and wall shear
+// (calcTauWall, main_v1.9.f90:930-977).  Blocks 0..n3-1: plane k=b+1;
+// block n3: tauL; block n3+1: tauU.  Fixed-order reductions: deterministic.
+constexpr int kStatThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const double *q, int do_moments,
+                                                        int do_tau)
+{
+    __shared__ double red[kStatThreads / 32][23];
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (frozen(P.status, P.step + 1)) return;
+    if (b < n3) {
+        if (!do_moments) return;
+        const int k = b + 1;
+        double acc[23];
+#pragma unroll
+        for (int c = 0; c < 23; c++) acc[c] = 0.0;
+        const int np = n1 * n2;
+        for (int p = tid; p < np; p += kStatThreads) {
+            const int jj = p / n1, ii = p - jj * n1;
+            double x[7];
+            ref_var(P, q, ii + 1, jj + 1, k, x);
+#pragma unroll
+            for (int m = 0; m < 7; m++) {
+                acc[m] += x[m];
+                acc[7 + m] += x[m] * x[m];
+            }
+            acc[14] += x[0] * x[3];
+            acc[15] += x[0] * x[5];
+            acc[16] += x[1] * x[2];
+            acc[17] += x[1] * x[3];
+            acc[18] += x[2] * x[3];
+            acc[19] += x[2] * x[5];
+            acc[20] += x[5] * x[3];
+            acc[21] += x[6] * x[3];
+            acc[22] += x[6] * x[5];
+        }
+#pragma unroll
+        for (int c = 0; c < 23; c++) {
+            const double s = warp_sum(acc[c]);
+            if (lane == 0) red[warp][c] = s;
+        }
+        __syncthreads();
+        if (tid < 23) {
+            double s = 0.0;
+            for (int w = 0; w < kStatThreads / 32; w++) s += red[w][tid];
+            const double nxy = (double)(n1 * n2);
+            double *out;
+            if (tid < 7) out = P.stat + (size_t)tid * n3;
+            else if (tid < 14) out = P.stat + (size_t)7 * n3 + (size_t)(tid - 7) * n3;
+            else out = P.stat + (size_t)14 * n3 + (size_t)(tid - 14) * n3;
+            out[k - 1] = s / nxy;
+        }
+        return;
+    }
+    if (!do_tau) return;
+    const int wall = b - n3;
+    const double *W = P.wp + (size_t)wall * 8 * P.plane;
+    const double *c = wall == 0 ? P.f1 : P.b1;
+    const int k2 = wall == 0 ? 2 : n3 - 1, k3 = wall == 0 ? 3 : n3 - 2;
+    double acc = 0.0;
+    const int ni = n1 - 2, np = (n1 - 2) * (n2 - 2);
+    for (int p = tid; p < np; p += kStatThreads) {
+        const int jj = 2 + p / ni, ii = 2 + p % ni;
+        const long long o = (long long)jj * P.px + ii;
+        const double mu = W[7 * P.plane + o];
+        const double dwdx = ((mu * (W[3 * P.plane + o + 1] - W[3 * P.plane + o - 1])) * 0.5) * P.invdx;
+        const long long o2 = (long long)k2 * P.plane + o, o3 = (long long)k3 * P.plane + o;
+        const double u2 = q[P.vol + o2] / q[o2];
+        const double u3 = q[P.vol + o3] / q[o3];
+        const double dudz = mu * ((c[0] * W[1 * P.plane + o] + c[1] * u2) + c[2] * u3);
+        acc += (dwdx + dudz) * P.invRe;
+    }
+    const double s = warp_sum(acc);
+    if (lane == 0) red[warp][0] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kStatThreads / 32; w++) t += red[w][0];
+        P.stat[(size_t)23 * n3 + wall] = t / (double)np;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Upload: var(1:nP1,1:nP2,1:nP3,1:7) (device copy, [m][k][j][i]) -> state.
+// initSolV (main_v1.9.f90:284-294): Q = rho*(1,u,v,w,E) at every point.
+__global__ void k_upload(const KParams P, const double *var, double *qa, double *qb, double *qc, double *cs)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const long long N = (long long)n1 * n2 * n3;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int ii = (int)(p % n1);
+        const int jj = (int)((p / n1) % n2);
+        const int kk = (int)(p / ((long long)n1 * n2));
+        const int i = ii + 1, j = jj + 1, k = kk + 1;
+        double x[7];
+#pragma unroll
+        for (int m = 0; m < 7; m++) x[m] = var[(size_t)m * N + p];
+        const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+        double q[5] = {x[0], x[0] * x[1], x[0] * x[2], x[0] * x[3], x[0] * x[4]};
+#pragma unroll
+        for (int c = 0; c < 5; c++) qa[c * P.vol + o] = q[c];
+        if (k == 1 || k == n3) {
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                qb[c * P.vol + o] = q[c];
+                if (qc) qc[c * P.vol + o] = q[c];
+            }
+            double *W = P.wp + (size_t)(k == 1 ? 0 : 8) * P.plane + (long long)j * P.px + i;
+#pragma unroll
+            for (int m = 0; m < 7; m++) W[(size_t)m * P.plane] = x[m];
+            W[(size_t)7 * P.plane] = pow(x[5], 0.7);
+        } else if ((i == 1 || i == n1) && (j == 1 || j == n2)) {
+            const int c = (i == 1 ? 0 : 1) + (j == 1 ? 0 : 2);
+#pragma unroll
+            for (int m = 0; m < 7; m++) cs[((size_t)k * 4 + c) * 7 + m] = x[m];
+        }
+    }
+}
+
+// periodic images of Q for interior planes (the reference's initial share2P,
+// including corner images so every periodic read is consistent); and of the
+// wall planes' primitive ring i,j in {0, nP+1}
+__device__ __forceinline__ int wrap_idx(int i, int n)
+{
+    if (i == 0) return n - 2;
+    if (i == 1) return n - 1;
+    if (i == n) return 2;
+    if (i == n + 1) return 3;
+    return i;
+}
+
+__global__ void k_fill_ghosts(const KParams P, double *q)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 2 + blockIdx.z;
+    const int n1 = P.n1, n2 = P.n2;
+    if (i > n1 + 1 || j > n2 + 1) return;
+    const int si = wrap_idx(i, n1), sj = wrap_idx(j, n2);
+    if (si == i && sj == j) return;
+    const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+    const long long s = (long long)k * P.plane + (long long)sj * P.px + si;
+#pragma unroll
+    for (int c = 0; c < 5; c++) q[c * P.vol + o] = q[c * P.vol + s];
+}
+
+__global__ void k_fill_wall_ring(const KParams P)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int wall = blockIdx.z;
+    const int n1 = P.n1, n2 = P.n2;
+    if (i > n1 + 1 || j > n2 + 1) return;
+    if (i >= 1 && i <= n1 && j >= 1 && j <= n2) return;
+    const int si = (i == 0 || i == n1 + 1) ? wrap_idx(i, n1) : i;
+    const int sj = (j == 0 || j == n2 + 1) ? wrap_idx(j, n2) : j;
+    double *W = P.wp + (size_t)wall * 8 * P.plane;
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+        W[(size_t)m * P.plane + (long long)j * P.px + i] = W[(size_t)m * P.plane + (long long)sj * P.px + si];
+}
+
+// Download: state -> var(1:nP1,1:nP2,1:nP3,1:7) ([m][k][j][i])
+__global__ void k_download(const KParams P, const double *q, double *var)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const long long N = (long long)n1 * n2 * n3;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int ii = (int)(p % n1);
+        const int jj = (int)((p / n1) % n2);
+        const int kk = (int)(p / ((long long)n1 * n2));
+        double x[7];
+        ref_var(P, q, ii + 1, jj + 1, kk + 1, x);
+#pragma unroll
+        for (int m = 0; m < 7; m++) var[(size_t)m * N + p] = x[m];
+    }
+}
+
+// checkSoln over every point (main_v1.9.f90:729-740)
+__global__ void k_check(const KParams P, const double *q)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const long long N = (long long)n1 * n2 * n3;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int ii = (int)(p % n1);
+        const int jj = (int)((p / n1) % n2);
+        const int kk = (int)(p / ((long long)n1 * n2));
+        double x[7];
+        ref_var(P, q, ii + 1, jj + 1, kk + 1, x);
+        if (x[0] < 0.0 || x[5] < 0.0) flag_blown(P.status, ii + 1, jj + 1, kk + 1, P.step);
+    }
+}
+
+}  // namespace chan

@@ -1,0 +1,586 @@
+// chanrhs.cu -- host side of the C ABI declared in include/chanrhs.h.
+//
+// The context owns every device buffer; host arrays are only read or
+// written inside chan_upload, chan_download and chan_stats.  All work is
+// queued on one CUDA stream per context.
+#include "chanrhs.h"
+#include "chan_kernels.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr int TI = 32;  // stage-kernel tile: 32 columns in x (one warp row)
+constexpr int TJ = 8;   // 8 rows in y -> 256 threads, 2 CTAs per SM
+
+std::string g_init_error;
+
+struct ProfPair {
+    int cls;
+    cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct chan_ctx {
+    chan_params p{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    chan::KParams kp{};
+    double *q[3] = {nullptr, nullptr, nullptr};
+    double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr;
+    chan::DevStatus *status = nullptr;
+    chan::DevStatus *h_status = nullptr;
+    int n1 = 0, n2 = 0, n3 = 0, px = 0, NJ = 0;
+    long long plane = 0, vol = 0;
+    int ntx = 0, nty = 0, nchunks = 1, kchunk = 1;
+    int nstage = 2;
+    int cur = 0;             // buffer holding the latest state
+    bool uploaded = false;
+    long long nstep = 0;
+    double time = 0.0;
+    long long sync_nstep = 0;  // counters at the last status read without a blow-up
+    double sync_time = 0.0;
+    std::string err;
+    bool prof = false;
+    std::vector<ProfPair> prof_pairs;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t dev_bytes = 0;
+};
+
+namespace {
+
+int fail(chan_ctx *c, const char *what, cudaError_t e)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    if (c) c->err = buf; else g_init_error = buf;
+    return CHAN_ECUDA;
+}
+
+#define CK(c, call)                                   \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return fail((c), #call, e_); \
+    } while (0)
+
+cudaEvent_t get_event(chan_ctx *c)
+{
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// bracket a launch with events when profiling is on
+struct ProfScope {
+    chan_ctx *c;
+    int cls;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ProfScope(chan_ctx *c_, int cls_) : c(c_), cls(cls_)
+    {
+        if (c->prof) {
+            a = get_event(c);
+            b = get_event(c);
+            if (a) cudaEventRecord(a, c->stream);
+        }
+    }
+    ~ProfScope()
+    {
+        if (c->prof && a && b) {
+            cudaEventRecord(b, c->stream);
+            c->prof_pairs.push_back({cls, a, b});
+        }
+    }
+};
+
+// one-sided wall coefficients, v1.10/codes/main_v1.9.f90:59-83 (x3 1-based)
+void wall_coeffs(const double *x3, int n3, double out[14])
+{
+    const double one = 1.0, haf = 0.5;
+    double dz1 = x3[2] - x3[1];
+    double alpha = (x3[3] - x3[2]) / dz1;
+    double t = dz1 * alpha * (alpha + one);
+    out[0] = (one - (alpha + one) * (alpha + one)) / t;
+    out[1] = ((alpha + one) * (alpha + one)) / t;
+    out[2] = -one / t;
+    t = haf * (dz1 * dz1) * alpha * (alpha + one);
+    out[3] = alpha / t;
+    out[4] = -(alpha + one) / t;
+    out[5] = one / t;
+    double dzN = x3[n3] - x3[n3 - 1];
+    alpha = (x3[n3 - 1] - x3[n3 - 2]) / dzN;
+    t = dzN * alpha * (alpha + one);
+    out[6] = ((alpha + one) * (alpha + one) - one) / t;
+    out[7] = -((alpha + one) * (alpha + one)) / t;
+    out[8] = one / t;
+    t = haf * (dzN * dzN) * alpha * (alpha + one);
+    out[9] = alpha / t;
+    out[10] = -(alpha + one) / t;
+    out[11] = one / t;
+    out[12] = dz1;
+    out[13] = dzN;
+}
+
+void set_stage(chan_ctx *c, int iter)
+{
+    chan::KParams &k = c->kp;
+    const double dt = c->p.dt;
+    if (c->nstage == 3) {
+        if (iter == 1) {
+            k.qin = c->q[0]; k.qbase = c->q[0]; k.qout = c->q[1];
+            k.rk_mode = 0; k.rk_a = 0.0; k.rk_b = 1.0; k.rk_cdt = dt;
+        } else if (iter == 2) {
+            k.qin = c->q[1]; k.qbase = c->q[0]; k.qout = c->q[2];
+            k.rk_mode = 2; k.rk_a = 0.75; k.rk_b = 0.25; k.rk_cdt = 0.25 * dt;
+        } else {
+            k.qin = c->q[2]; k.qbase = c->q[0]; k.qout = c->q[0];
+            k.rk_mode = 2; k.rk_a = 1.0 / 3.0; k.rk_b = 2.0 / 3.0; k.rk_cdt = (2.0 / 3.0) * dt;
+        }
+    } else {
+        if (iter == 1) {
+            // solV(:,2)=solV(:,1); solV(:,1)+=haf*dt*R  (main_v1.9.f90:575-578)
+            k.qin = c->q[0]; k.qbase = c->q[0]; k.qout = c->q[1];
+            k.rk_mode = 0; k.rk_a = 0.0; k.rk_b = 1.0; k.rk_cdt = 0.5 * dt;
+        } else {
+            // solV(:,1)=solV(:,2)+dt*R  (main_v1.9.f90:580-582)
+            k.qin = c->q[1]; k.qbase = c->q[0]; k.qout = c->q[0];
+            k.rk_mode = 1; k.rk_a = 1.0; k.rk_b = 0.0; k.rk_cdt = dt;
+        }
+    }
+}
+
+int launch_stage(chan_ctx *c, int iter, bool check, long long step)
+{
+    set_stage(c, iter);
+    c->cur = c->kp.qout == c->q[0] ? 0 : (c->kp.qout == c->q[1] ? 1 : 2);
+    c->kp.check = check ? 1 : 0;
+    c->kp.step = step;
+    {
+        ProfScope ps(c, 0);
+        dim3 grid(c->ntx, c->nty, c->nchunks), block(TI, TJ);
+        chan::k_stage<TI, TJ><<<grid, block, chan::StageShape<TI, TJ>::bytes, c->stream>>>(c->kp);
+    }
+    CK(c, cudaGetLastError());
+    {
+        ProfScope ps(c, 1);
+        dim3 block(32, 8), grid((c->n1 + 2 + 31) / 32, (c->n2 + 2 + 7) / 8, 2);
+        chan::k_wall<<<grid, block, 0, c->stream>>>(c->kp);
+    }
+    CK(c, cudaGetLastError());
+    return CHAN_OK;
+}
+
+int launch_stats(chan_ctx *c, long long step, int moments, int tau)
+{
+    c->kp.step = step;
+    ProfScope ps(c, 2);
+    chan::k_stats<<<c->n3 + 2, chan::kStatThreads, 0, c->stream>>>(c->kp, c->q[c->cur], moments, tau);
+    CK(c, cudaGetLastError());
+    return CHAN_OK;
+}
+
+// queue nsteps steps; host counters advance optimistically
+int enqueue_steps(chan_ctx *c, int nsteps)
+{
+    for (int s = 0; s < nsteps; s++) {
+        const long long step = c->nstep + 1;
+        for (int it = 1; it <= c->nstage; it++) {
+            int r = launch_stage(c, it, it == c->nstage, step);
+            if (r) return r;
+        }
+        if (c->p.istat > 0 && step % c->p.istat == 0) {
+            int r = launch_stats(c, step, 1, 1);
+            if (r) return r;
+        }
+        c->nstep = step;
+        c->time = c->time + c->p.dt;
+    }
+    return CHAN_OK;
+}
+
+// read the device status; resolve the step/time of a blow-up
+int read_status(chan_ctx *c, int32_t *ijk)
+{
+    CK(c, cudaMemcpyAsync(c->h_status, c->status, sizeof(chan::DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    const chan::DevStatus &s = *c->h_status;
+    if (s.blown) {
+        if (s.blown_step < c->nstep && s.blown_step > c->sync_nstep) {
+            // counters of the step that blew up, accumulated as the time loop does
+            double t = c->sync_time;
+            for (long long n = c->sync_nstep; n < s.blown_step; n++) t = t + c->p.dt;
+            c->time = t;
+            c->nstep = s.blown_step;
+        }
+        if (ijk) { ijk[0] = s.ijk[0]; ijk[1] = s.ijk[1]; ijk[2] = s.ijk[2]; }
+        return CHAN_BLOWUP;
+    }
+    if (s.nonfinite) {
+        if (ijk) { ijk[0] = s.nf_ijk[0]; ijk[1] = s.nf_ijk[1]; ijk[2] = s.nf_ijk[2]; }
+        return CHAN_NONFINITE;
+    }
+    if (ijk) ijk[0] = ijk[1] = ijk[2] = 0;
+    c->sync_nstep = c->nstep;
+    c->sync_time = c->time;
+    return CHAN_OK;
+}
+
+int dalloc(chan_ctx *c, double **p, size_t n)
+{
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(double));
+    if (e != cudaSuccess) {
+        fail(c, "cudaMalloc", e);
+        return CHAN_ENOMEM;
+    }
+    c->dev_bytes += n * sizeof(double);
+    e = cudaMemsetAsync(*p, 0, n * sizeof(double), c->stream);
+    if (e != cudaSuccess) return fail(c, "cudaMemsetAsync", e);
+    return CHAN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *chan_version(void) { return "compchan3dmpi_b200 0.1 (sm_100a, fp64)"; }
+
+const char *chan_last_error(chan_ctx *c)
+{
+    if (!c) return g_init_error.c_str();
+    return c->err.c_str();
+}
+
+int chan_init(const chan_params *p, const double *x3, const double *jac, const double *invJac, chan_ctx **out)
+{
+    g_init_error.clear();
+    if (!out) { g_init_error = "out is NULL"; return CHAN_EINVAL; }
+    *out = nullptr;
+    if (!p || !x3 || !jac || !invJac) { g_init_error = "NULL argument"; return CHAN_EINVAL; }
+    if (p->nP[0] < 6 || p->nP[1] < 6 || p->nP[2] < 6) { g_init_error = "every nP must be >= 6"; return CHAN_EINVAL; }
+    if ((long long)p->nP[0] * p->nP[1] * p->nP[2] > (1LL << 31)) { g_init_error = "grid too large"; return CHAN_EINVAL; }
+    if (!(p->Re > 0) || !(p->Mac > 0) || !(p->dt > 0) || !(p->Pr > 0) || !(p->gama > 1)) {
+        g_init_error = "Re, Mac, dt, Pr must be > 0 and gama > 1";
+        return CHAN_EINVAL;
+    }
+    if (p->rk_scheme != CHAN_RK2 && p->rk_scheme != CHAN_RK3) { g_init_error = "rk_scheme must be 2 or 3"; return CHAN_EINVAL; }
+    if (p->forcing != CHAN_FORCE_WALLSHEAR && p->forcing != CHAN_FORCE_NONE) { g_init_error = "bad forcing"; return CHAN_EINVAL; }
+    if (p->flags != 0) { g_init_error = "flags must be 0"; return CHAN_EINVAL; }
+    if (p->istat < 0) { g_init_error = "istat must be >= 0"; return CHAN_EINVAL; }
+    for (int k = 1; k < p->nP[2]; k++)
+        if (!(x3[k] > x3[k - 1])) { g_init_error = "x3 must increase"; return CHAN_EINVAL; }
+
+    chan_ctx *c = new chan_ctx();
+    c->p = *p;
+    c->dev = p->device;
+    cudaError_t e = cudaSetDevice(c->dev);
+    if (e != cudaSuccess) { fail(nullptr, "cudaSetDevice", e); delete c; return CHAN_ECUDA; }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { fail(nullptr, "cudaStreamCreate", e); delete c; return CHAN_ECUDA; }
+
+    const int n1 = p->nP[0], n2 = p->nP[1], n3 = p->nP[2];
+    c->n1 = n1; c->n2 = n2; c->n3 = n3;
+    c->px = ((n1 + 2) + 7) / 8 * 8;
+    c->NJ = n2 + 2;
+    c->plane = (long long)c->px * c->NJ;
+    c->vol = c->plane * (n3 + 2);
+    c->nstage = p->rk_scheme == CHAN_RK3 ? 3 : 2;
+
+    int r;
+    for (int b = 0; b < 3; b++)
+        if ((r = dalloc(c, &c->q[b], 5 * (size_t)c->vol))) { g_init_error = c->err; chan_free(c); return r; }
+    if ((r = dalloc(c, &c->wp, 2 * 8 * (size_t)c->plane)) || (r = dalloc(c, &c->cs, (size_t)(n3 + 2) * 28)) ||
+        (r = dalloc(c, &c->tabs, 4 * (size_t)(n3 + 2))) || (r = dalloc(c, &c->stat, 23 * (size_t)n3 + 2)) ||
+        (r = dalloc(c, &c->dvar, 7 * (size_t)n1 * n2 * n3))) {
+        g_init_error = c->err;
+        chan_free(c);
+        return r;
+    }
+    e = cudaMalloc((void **)&c->status, sizeof(chan::DevStatus));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->status, 0, sizeof(chan::DevStatus), c->stream);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_status, sizeof(chan::DevStatus));
+    if (e != cudaSuccess) { fail(nullptr, "status allocation", e); chan_free(c); return CHAN_ENOMEM; }
+
+    // mesh-derived tables (1-based k stored at index k)
+    std::vector<double> X3(n3 + 1), JAC(n3 + 1), INV(n3 + 1);
+    for (int k = 1; k <= n3; k++) { X3[k] = x3[k - 1]; JAC[k] = jac[k - 1]; INV[k] = invJac[k - 1]; }
+    double co[14];
+    wall_coeffs(X3.data(), n3, co);
+
+    const double Re = p->Re, Mac = p->Mac, gama = p->gama;
+    const double dx = p->Lx / (double)(n1 - 1), dy = p->Ly / (double)(n2 - 1), dXi = 2.0 / (double)(n3 - 1);
+    const double invdx = 1.0 / dx, invdy = 1.0 / dy, invdXi = 1.0 / dXi;
+    std::vector<double> tab(4 * (size_t)(n3 + 2), 0.0);
+    for (int k = 1; k <= n3; k++) {
+        tab[0 * (n3 + 2) + k] = 0.5 * invdXi * INV[k];
+        tab[1 * (n3 + 2) + k] = (invdXi * INV[k]) / 8.0;
+        tab[2 * (n3 + 2) + k] = (invdXi * INV[k]) * (1.0 / 12.0);
+        tab[3 * (n3 + 2) + k] = (Re * dXi) * JAC[k];
+    }
+    e = cudaMemcpyAsync(c->tabs, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) { fail(nullptr, "table upload", e); chan_free(c); return CHAN_ECUDA; }
+
+    chan::KParams &k = c->kp;
+    k.n1 = n1; k.n2 = n2; k.n3 = n3; k.px = c->px; k.NJ = c->NJ;
+    k.plane = c->plane; k.vol = c->vol;
+    k.wp = c->wp; k.cs = c->cs;
+    k.czh = c->tabs; k.cz8 = c->tabs + (n3 + 2); k.cz12 = c->tabs + 2 * (n3 + 2); k.pez = c->tabs + 3 * (n3 + 2);
+    k.stat = c->stat; k.status = c->status;
+    k.invRe = 1.0 / Re;
+    k.ggM = gama * (gama - 1) * (Mac * Mac);
+    k.ggMh = k.ggM * 0.5;
+    k.gM2 = gama * (Mac * Mac);
+    k.inv_gM2 = 1.0 / k.gM2;
+    k.kq = gama * k.invRe * (1.0 / p->Pr);
+    k.two3rd = 2.0 / 3.0;
+    k.invdx = invdx; k.invdy = invdy;
+    k.hdx = 0.5 * invdx; k.hdy = 0.5 * invdy;
+    k.sx8 = invdx / 8.0; k.sx12 = invdx * (1.0 / 12.0);
+    k.sy8 = invdy / 8.0; k.sy12 = invdy * (1.0 / 12.0);
+    k.pex = Re * dx; k.pey = Re * dy;
+    k.PexVal = p->Pe[0]; k.PeyVal = p->Pe[1]; k.pez_val = p->Pe[2];
+    k.inv_dz1 = 1.0 / co[12]; k.inv_dzN = 1.0 / co[13];
+    k.Twb = p->Tw[0]; k.Twt = p->Tw[1];
+    k.muwb = pow(p->Tw[0], 0.7); k.muwt = pow(p->Tw[1], 0.7);
+    for (int m = 0; m < 3; m++) {
+        k.f1[m] = co[m]; k.f2[m] = co[3 + m]; k.b1[m] = co[6 + m]; k.b2[m] = co[9 + m];
+    }
+    k.force_on = p->forcing == CHAN_FORCE_WALLSHEAR ? 1 : 0;
+
+    // stage-kernel launch shape: tiles x k-chunks filling whole waves
+    c->ntx = (n1 - 2 + TI - 1) / TI;
+    c->nty = (n2 - 2 + TJ - 1) / TJ;
+    const size_t smem = chan::StageShape<TI, TJ>::bytes;
+    e = cudaFuncSetAttribute(chan::k_stage<TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) { fail(nullptr, "cudaFuncSetAttribute", e); chan_free(c); return CHAN_ECUDA; }
+    int sms = 148, occ = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ>, TI * TJ, smem);
+    if (occ < 1) occ = 1;
+    const long long slots = (long long)sms * occ;
+    const int nz = n3 - 2;
+    const long long tiles = (long long)c->ntx * c->nty;
+    double best = -1.0;
+    int bestc = 1;
+    for (int nc = 1; nc <= nz; nc++) {
+        const int chunk = (nz + nc - 1) / nc;
+        const int nce = (nz + chunk - 1) / chunk;
+        if (nce != nc) continue;
+        const long long ctas = tiles * nc;
+        const long long waves = (ctas + slots - 1) / slots;
+        const double eff = (double)ctas / (double)(waves * slots) * (double)chunk / (chunk + 2.5);
+        if (eff > best + 1e-9) { best = eff; bestc = nc; }
+    }
+    c->nchunks = bestc;
+    c->kchunk = (nz + bestc - 1) / bestc;
+    k.kchunk = c->kchunk;
+
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { fail(nullptr, "init sync", e); chan_free(c); return CHAN_ECUDA; }
+    *out = c;
+    return CHAN_OK;
+}
+
+int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time)
+{
+    if (!c || !var) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t N = (size_t)c->n1 * c->n2 * c->n3;
+    CK(c, cudaMemcpyAsync(c->dvar, var, 7 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    chan::k_upload<<<1184, 256, 0, c->stream>>>(c->kp, c->dvar, c->q[0], c->q[1], c->q[2], c->cs);
+    CK(c, cudaGetLastError());
+    {
+        dim3 block(32, 8), grid((c->n1 + 2 + 31) / 32, (c->n2 + 2 + 7) / 8, c->n3 - 2);
+        chan::k_fill_ghosts<<<grid, block, 0, c->stream>>>(c->kp, c->q[0]);
+        CK(c, cudaGetLastError());
+        dim3 g2((c->n1 + 2 + 31) / 32, (c->n2 + 2 + 7) / 8, 2);
+        chan::k_fill_wall_ring<<<g2, block, 0, c->stream>>>(c->kp);
+        CK(c, cudaGetLastError());
+    }
+    CK(c, cudaMemsetAsync(c->stat, 0, (23 * (size_t)c->n3 + 2) * sizeof(double), c->stream));
+    CK(c, cudaMemsetAsync(c->status, 0, sizeof(chan::DevStatus), c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->nstep = nstep;
+    c->time = time;
+    c->sync_nstep = nstep;
+    c->sync_time = time;
+    c->cur = 0;
+    c->uploaded = true;
+    return CHAN_OK;
+}
+
+int chan_stage(chan_ctx *c, int iter)
+{
+    if (!c) return CHAN_EINVAL;
+    if (!c->uploaded) { c->err = "chan_stage before chan_upload"; return CHAN_ESTATE; }
+    if (iter < 1 || iter > c->nstage) { c->err = "iter out of range"; return CHAN_EINVAL; }
+    CK(c, cudaSetDevice(c->dev));
+    int r = launch_stage(c, iter, iter == c->nstage, c->nstep + 1);
+    if (r) return r;
+    return read_status(c, nullptr);
+}
+
+int chan_step_async(chan_ctx *c, int nsteps)
+{
+    if (!c || nsteps < 0) return CHAN_EINVAL;
+    if (!c->uploaded) { c->err = "chan_step before chan_upload"; return CHAN_ESTATE; }
+    CK(c, cudaSetDevice(c->dev));
+    return enqueue_steps(c, nsteps);
+}
+
+int chan_step(chan_ctx *c, int nsteps)
+{
+    int r = chan_step_async(c, nsteps);
+    if (r) return r;
+    return read_status(c, nullptr);
+}
+
+int chan_check(chan_ctx *c)
+{
+    if (!c) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    c->kp.step = c->nstep;
+    chan::k_check<<<1184, 256, 0, c->stream>>>(c->kp, c->q[c->cur]);
+    CK(c, cudaGetLastError());
+    return read_status(c, nullptr);
+}
+
+int chan_tau_wall(chan_ctx *c)
+{
+    if (!c) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    int r = launch_stats(c, c->nstep, 0, 1);
+    if (r) return r;
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_avg_spatial(chan_ctx *c)
+{
+    if (!c) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    int r = launch_stats(c, c->nstep, 1, 0);
+    if (r) return r;
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_stats(chan_ctx *c, double *tau2, double *stat1, double *stat2, double *corr)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t n3 = (size_t)c->n3;
+    if (tau2) CK(c, cudaMemcpyAsync(tau2, c->stat + 23 * n3, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (stat1) CK(c, cudaMemcpyAsync(stat1, c->stat, 7 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (stat2) CK(c, cudaMemcpyAsync(stat2, c->stat + 7 * n3, 7 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (corr) CK(c, cudaMemcpyAsync(corr, c->stat + 14 * n3, 9 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_set_forcing(chan_ctx *c, double tauL, double tauU, const double *rhobar)
+{
+    if (!c || !rhobar) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t n3 = (size_t)c->n3;
+    double tau[2] = {tauL, tauU};
+    CK(c, cudaMemcpyAsync(c->stat + 23 * n3, tau, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(c->stat, rhobar, n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_download(chan_ctx *c, double *var)
+{
+    if (!c || !var) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t N = (size_t)c->n1 * c->n2 * c->n3;
+    chan::k_download<<<1184, 256, 0, c->stream>>>(c->kp, c->q[c->cur], c->dvar);
+    CK(c, cudaGetLastError());
+    CK(c, cudaMemcpyAsync(var, c->dvar, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_status(chan_ctx *c, int32_t *ijk, int64_t *nstep, double *time)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    int r = read_status(c, ijk);
+    if (nstep) *nstep = c->nstep;
+    if (time) *time = c->time;
+    return r;
+}
+
+int chan_sync(chan_ctx *c)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    return read_status(c, nullptr);
+}
+
+int chan_profile(chan_ctx *c, int enable)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaStreamSynchronize(c->stream));
+    for (auto &pp : c->prof_pairs) { c->ev_pool.push_back(pp.a); c->ev_pool.push_back(pp.b); }
+    c->prof_pairs.clear();
+    c->prof = enable != 0;
+    return CHAN_OK;
+}
+
+int chan_profile_read(chan_ctx *c, double *ms3, int64_t *count3)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaStreamSynchronize(c->stream));
+    double ms[3] = {0, 0, 0};
+    int64_t cnt[3] = {0, 0, 0};
+    for (auto &pp : c->prof_pairs) {
+        float t = 0.f;
+        CK(c, cudaEventElapsedTime(&t, pp.a, pp.b));
+        ms[pp.cls] += t;
+        cnt[pp.cls] += 1;
+    }
+    for (int m = 0; m < 3; m++) {
+        if (ms3) ms3[m] = ms[m];
+        if (count3) count3[m] = cnt[m];
+    }
+    return CHAN_OK;
+}
+
+void *chan_stream(chan_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int64_t chan_device_bytes(chan_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
+
+void chan_free(chan_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &pp : c->prof_pairs) { cudaEventDestroy(pp.a); cudaEventDestroy(pp.b); }
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    for (int b = 0; b < 3; b++) if (c->q[b]) cudaFree(c->q[b]);
+    if (c->wp) cudaFree(c->wp);
+    if (c->cs) cudaFree(c->cs);
+    if (c->tabs) cudaFree(c->tabs);
+    if (c->stat) cudaFree(c->stat);
+    if (c->dvar) cudaFree(c->dvar);
+    if (c->status) cudaFree(c->status);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+/*
+ * chanrhs.h -- C ABI of the B200 time-step library for the compressible
+ * channel solver theparvezahmad/compChan3Dmpi.
+ *
+ * The library replaces the reference's per-stage and per-step subroutines.
+ * The reference calls them from its main program, v1.10/codes/main_v1.10.f90:20-53
+ * (module bodies in v1.10/codes/module_comp.f90).  The monolithic form is
+ * v1.9/codes/main_v1.9.f90:304-1049.
+ * All entry points use plain pointers, sizes and C scalars, so a Fortran host
+ * can bind them with iso_c_binding.  INTEGRATION.md gives the interface module.
+ *
+ * Axes and arrays follow the reference exactly.
+ *   index 1 (i, nP[0]) : streamwise x, periodic.
+ *   index 2 (j, nP[1]) : spanwise, periodic.
+ *   index 3 (k, nP[2]) : wall-normal, stretched, isothermal no-slip walls at k=1 and k=nP3.
+ * Periodic directions store both duplicate end points, as in
+ * v1.9/codes/comdata.f90:85-86, so there are nP-2 unique points.
+ * `var` is the reference array var(1:nP1,1:nP2,1:nP3,1:7) (v1.9/codes/main_v1.9.f90:38).
+ * It is column-major (i fastest) and holds rho,u,v,w,E,T,p.
+ *
+ * Ownership: the caller owns every host array.  The library owns all device
+ * memory, copies host data only inside chan_upload / chan_download /
+ * chan_stats, and never keeps a host pointer.
+ * Threading: one context per CUDA stream; a context is not thread-safe.
+ * Return codes: 0 OK; negative = usage/IO/CUDA error; positive = numerical status.
+ */
+#ifndef CHANRHS_H
+#define CHANRHS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAN_OK 0
+#define CHAN_BLOWUP 1      /* rho<0 or T<0 after a step (v1.9/codes/main_v1.9.f90:709-743) */
+#define CHAN_NONFINITE 2   /* NaN or Inf met in the updated state */
+#define CHAN_EINVAL (-1)   /* bad argument */
+#define CHAN_ENOMEM (-2)   /* device allocation failed */
+#define CHAN_ECUDA (-3)    /* CUDA runtime error (see chan_last_error) */
+#define CHAN_ESTATE (-4)   /* call out of order (e.g. step before upload) */
+
+#define CHAN_RK2 2         /* the reference's midpoint RK2: maxiter=2, v1.9/codes/comdata.f90:8 */
+#define CHAN_RK3 3         /* SSP-RK3 (Shu-Osher); no reference counterpart */
+
+#define CHAN_FORCE_WALLSHEAR 0  /* reference forcing 0.5*(tauL-tauU)*rhobar(k), lagged (main_v1.9.f90:547-553) */
+#define CHAN_FORCE_NONE 1       /* no source term */
+
+/* Run-time parameters.  Field-for-field equivalent of the reference's
+ * compile-time constants and param.dat deck (v1.9/codes/comdata.f90:4-68). */
+typedef struct chan_params {
+    int32_t nP[3];      /* nP(1..3) grid points including walls and periodic duplicates */
+    int32_t istat;      /* cadence of wall-shear/plane statistics (param.dat field) */
+    int32_t rk_scheme;  /* CHAN_RK2 (reference) or CHAN_RK3 */
+    int32_t forcing;    /* CHAN_FORCE_WALLSHEAR (reference) or CHAN_FORCE_NONE */
+    int32_t device;     /* CUDA device ordinal */
+    int32_t flags;      /* reserved, must be 0 */
+    double Re;          /* Reynolds number (param.dat) */
+    double Mac;         /* Mach number (param.dat) */
+    double dt;          /* time step (param.dat) */
+    double Pr;          /* Prandtl number; the reference hardcodes 0.71 (comdata.f90:12) */
+    double gama;        /* ratio of specific heats, 1.4 (comdata.f90:11) */
+    double Pe[3];       /* PexVal, PeyVal, PezVal: QUICK/central switch thresholds */
+    double Lx, Ly;      /* periodic lengths x1(nP1), x2(nP2): 4*pi and 4*pi/3 (comdata.f90:81-82) */
+    double Tw[2];       /* wall temperature at k=1 and k=nP3; 1.0 in the reference (main_v1.9.f90:628) */
+} chan_params;
+
+typedef struct chan_ctx chan_ctx;
+
+/* Replaces readParam + setupMesh + the wall-coefficient block
+ * (v1.9/codes/comdata.f90:31-110, v1.9/codes/main_v1.9.f90:52-76;
+ *  v1.10: readParam, calcMeshParam, calcCoeffs, main_v1.10.f90:20-22).
+ * x3, jac and invJac are the wall-normal mesh arrays x3(1:nP3), jac(1:nP3)
+ * and invJac(1:nP3).  The wall-normal computational coordinate is uniform on [0,2]. */
+int chan_init(const chan_params *p, const double *x3, const double *jac,
+              const double *invJac, chan_ctx **out);
+
+/* Replaces readInputFile + initSolV + share2P(solV) + share2P(var)
+ * (v1.9/codes/main_v1.9.f90:210-301; main_v1.10.f90:25-29).
+ * var = var(1:nP1,1:nP2,1:nP3,1:7) read from the restart deck.
+ * The lagged forcing restarts at zero, as in the reference. */
+int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time);
+
+/* One Runge-Kutta stage.  Replaces calcFlux, calcSolV, share2P(solV),
+ * calcPrim, share2P(var) and calcBC (v1.9/codes/main_v1.9.f90:313-704;
+ * main_v1.10.f90:38-46).  iter is 1..2 for RK2 and 1..3 for RK3.  It does not
+ * advance nstep or time. */
+int chan_stage(chan_ctx *c, int iter);
+
+/* nsteps full time steps.  Each step increments nstep, adds dt to time, runs
+ * every stage, then the per-step tail in the reference's order: checkSoln,
+ * then calcTauWall and avgSpatial when mod(nstep,istat)==0
+ * (main_v1.9.f90:304-311, 709-1049; main_v1.10.f90:31-61).
+ * It stops after the step that blew up and returns CHAN_BLOWUP. */
+int chan_step(chan_ctx *c, int nsteps);
+
+/* Queue nsteps steps on the context's stream and return without waiting.
+ * Poll the result with chan_status.  The reference has no counterpart. */
+int chan_step_async(chan_ctx *c, int nsteps);
+
+/* checkSoln: rho<0 or T<0 anywhere (main_v1.9.f90:709-743; module_comp.f90:396). */
+int chan_check(chan_ctx *c);
+
+/* calcTauWall without its cadence test (main_v1.9.f90:910-967). */
+int chan_tau_wall(chan_ctx *c);
+
+/* avgSpatial without its cadence test (main_v1.9.f90:972-1002). */
+int chan_avg_spatial(chan_ctx *c);
+
+/* Copy out the forcing and statistics state.  Any pointer may be NULL.
+ * tau2[2]   = tauxzL, tauxzU.
+ * stat1[7*nP3], stat2[7*nP3] = stat1Spc(k,p), stat2Spc(k,p) stored as [p][k].
+ * corr[9*nP3] = corrSpc(k,c) stored as [c][k].
+ * Source: main_v1.9.f90:39-41, 1027-1037. */
+int chan_stats(chan_ctx *c, double *tau2, double *stat1, double *stat2, double *corr);
+
+/* Overwrite the lagged forcing state tauxzL, tauxzU and stat1Spc(:,1)
+ * (main_v1.9.f90:551-553).  rhobar has nP3 entries.  It is needed to
+ * restart with a non-zero forcing.  The reference has no counterpart. */
+int chan_set_forcing(chan_ctx *c, double tauL, double tauU, const double *rhobar);
+
+/* State back to var(1:nP1,1:nP2,1:nP3,1:7).  Used like writeSoln
+ * (main_v1.9.f90:749-794).  Corner duplicates and wall edge pressures hold
+ * the same stale values the reference's var holds. */
+int chan_download(chan_ctx *c, double *var);
+
+/* Blow-up / non-finite status.  Any pointer may be NULL.  ijk receives the
+ * 1-based (i,j,k) of one offending point.  nstep/time are the step counter
+ * and time of the last completed step. */
+int chan_status(chan_ctx *c, int32_t *ijk, int64_t *nstep, double *time);
+
+/* Block until queued work is done; return the status code as chan_status does. */
+int chan_sync(chan_ctx *c);
+
+/* Per-kernel device timing from CUDA events on the context's stream, for
+ * measurement tools.  enable=1 starts accumulating.
+ * chan_profile_read returns, per kernel class, the summed milliseconds and
+ * the launch count.  Classes: 0 stage, 1 wall BC, 2 statistics.  The
+ * reference has no counterpart. */
+int chan_profile(chan_ctx *c, int enable);
+int chan_profile_read(chan_ctx *c, double *ms3, int64_t *count3);
+
+/* The context's cudaStream_t (as void*), for callers that record events. */
+void *chan_stream(chan_ctx *c);
+
+/* Device bytes held by the context. */
+int64_t chan_device_bytes(chan_ctx *c);
+
+/* Last error message of this context, or of chan_init when c is NULL. */
+const char *chan_last_error(chan_ctx *c);
+
+/* Library version string. */
+const char *chan_version(void);
+
+/* Free device memory and the context.  NULL is allowed. */
+void chan_free(chan_ctx *c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHANRHS_H */

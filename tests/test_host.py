@@ -1,0 +1,111 @@
+"""CPU tests of the host-side pieces: seeded IC, mesh options, deck formats."""
+import math
+
+import numpy as np
+import pytest
+
+from compchan3dmpi_b200 import (ChanParams, laminar_noise, mesh_cosine, mesh_tanh, cfl_dt, periodic_coords,
+                                wall_coeffs)
+from compchan3dmpi_b200.deck import (fmt_e22_15, parse_fortran_real, quantize_deck, write_param_dat,
+                                     read_param_dat, write_3d_dat, read_3d_dat, DeckError)
+
+
+def test_ic_is_seeded_periodic_and_consistent():
+    p = ChanParams(nP=(18, 10, 13))
+    x3, _, _ = mesh_cosine(13)
+    a = laminar_noise(p, x3, seed=7)
+    b = laminar_noise(p, x3, seed=7)
+    c = laminar_noise(p, x3, seed=8)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    # periodic duplicates (mainV1.8_serial.f90:162-170)
+    assert np.array_equal(a[..., 0], a[..., -2]) and np.array_equal(a[..., -1], a[..., 1])
+    assert np.array_equal(a[:, :, 0], a[:, :, -2]) and np.array_equal(a[:, :, -1], a[:, :, 1])
+    # walls at rest, T = Tw
+    assert np.all(a[1:4, 0] == 0) and np.all(a[1:4, -1] == 0) and np.all(a[5, 0] == 1.0)
+    # equation of state and energy as main_v1.9.f90:605-606
+    np.testing.assert_allclose(a[6], a[0] * a[5] / (1.4 * 1.5 ** 2), rtol=1e-15)
+    ke = 0.5 * p.ggM * (a[1] ** 2 + a[2] ** 2 + a[3] ** 2)
+    np.testing.assert_allclose(a[4] - ke, a[5], rtol=1e-14)
+    # noise amplitude bounded by 10 % of the laminar profile
+    ulam = 1.5 * (1 - (x3 - 1) ** 2)
+    assert np.all(np.abs(a[2]) <= 0.1 * ulam[:, None, None] + 1e-15)
+
+
+def test_tanh_mesh():
+    x3, jac, inv = mesh_tanh(193, 2.2)
+    assert x3[0] == 0.0 and x3[-1] == 2.0 and np.all(np.diff(x3) > 0)
+    # analytic jacobian vs finite difference of the map
+    dxi = 2.0 / 192
+    fd = (x3[2:] - x3[:-2]) / (2 * dxi)
+    np.testing.assert_allclose(fd, jac[1:-1], rtol=2e-3)
+    np.testing.assert_allclose(inv, 1.0 / jac)
+    assert abs(np.sum(0.5 * (jac[1:] + jac[:-1])) * dxi - 2.0) < 1e-3
+
+
+def test_cfl_dt_scales_linearly():
+    p = ChanParams(nP=(16, 12, 17))
+    x3, jac, _ = mesh_cosine(17)
+    var = laminar_noise(p, x3)
+    d5 = cfl_dt(var, p, jac, 0.5)
+    d1 = cfl_dt(var, p, jac, 1.0)
+    assert d5 > 0 and abs(d1 / d5 - 2.0) < 1e-12
+
+
+def test_e22_15_format():
+    assert fmt_e22_15(0.0) == " 0.000000000000000E+00"
+    assert fmt_e22_15(1.0) == " 0.100000000000000E+01"
+    assert fmt_e22_15(-0.00123456789012345678) == "-0.123456789012346E-02"
+    assert len(fmt_e22_15(math.pi)) == 22
+    assert parse_fortran_real("0.314159265358979E+01") == 3.14159265358979
+    assert parse_fortran_real("0.1+100") == 1e99
+    q = quantize_deck(np.array([math.pi, -1e-7 / 3]))
+    assert q[0] == 3.14159265358979 and q[1] == float("-0.333333333333333E-07")
+
+
+def test_param_dat_roundtrip(tmp_path):
+    p = ChanParams(nP=(64, 48, 65), Re=3000.0, Mac=1.5, dt=1e-4, istat=10, Pe=(2.0, 2.0, 0.2))
+    f = tmp_path / "param.dat"
+    write_param_dat(f, p, descp="case4", topo=(2, 2, 2), inputPath="../input/3D.dat")
+    text = f.read_text().splitlines()
+    # values start at column 49 (48X in comdata.f90:37-55)
+    assert text[10][48:52] == "3000"[:4] or text[10][48:52].strip() == "3000."
+    q, ex = read_param_dat(f, nP=(64, 48, 65))
+    assert (q.Re, q.Mac, q.dt, q.istat, q.Pe) == (3000.0, 1.5, 1e-4, 10, (2.0, 2.0, 0.2))
+    assert ex["topo"] == (2, 2, 2) and ex["inputPath"] == "../input/3D.dat" and ex["descp"] == "case4"
+
+
+def test_param_dat_small_dt_uses_exponent(tmp_path):
+    p = ChanParams(dt=3.7e-5)
+    f = tmp_path / "param.dat"
+    write_param_dat(f, p)
+    q, _ = read_param_dat(f)
+    assert abs(q.dt - 3.7e-5) < 1e-10
+
+
+def test_3d_dat_roundtrip_and_errors(tmp_path):
+    p = ChanParams(nP=(6, 6, 7))
+    x3, _, _ = mesh_cosine(7)
+    v = quantize_deck(laminar_noise(p, x3))
+    f = tmp_path / "3D.dat"
+    write_3d_dat(f, v, periodic_coords(6, p.Lx), periodic_coords(6, p.Ly), x3, 1.25, 42)
+    back, t, n, x1, x2, x3b = read_3d_dat(f, p.nP)
+    assert np.array_equal(back, v) and t == 1.25 and n == 42
+    assert np.allclose(x3b, x3, atol=1e-6)
+    # a truncated file is reported with the record's indices, like the reference
+    lines = f.read_text().splitlines()
+    (tmp_path / "bad.dat").write_text("\n".join(lines[:40]) + "\n")
+    with pytest.raises(DeckError, match="Error in reading combined input file"):
+        read_3d_dat(tmp_path / "bad.dat", p.nP)
+    # a corrupt number too
+    bad = lines[:]
+    bad[10] = bad[10][:40] + "x" + bad[10][41:]
+    (tmp_path / "bad2.dat").write_text("\n".join(bad) + "\n")
+    with pytest.raises(DeckError):
+        read_3d_dat(tmp_path / "bad2.dat", p.nP)
+
+
+def test_wall_coeffs_sum_to_zero():
+    x3, _, _ = mesh_cosine(65)
+    c = wall_coeffs(x3)
+    assert abs(c["f1d2c0"] + c["f1d2c1"] + c["f1d2c2"]) < 1e-9 * abs(c["f1d2c0"])
+    assert abs(c["b1d2c0"] + c["b1d2c1"] + c["b1d2c2"]) < 1e-9 * abs(c["b1d2c0"])

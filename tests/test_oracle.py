@@ -1,0 +1,106 @@
+"""CPU tests of the oracle (the checker) against the reference's own data."""
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from compchan3dmpi_b200 import mesh_cosine, wall_coeffs
+
+GOLD = Path(__file__).with_name("golden")
+
+
+def test_fd_coeff_kat():
+    """Reference KAT: v1.8_validation/codes/nohupDebug.out:23-26.  The logged
+    values come from an ifort -O3 build; the near-wall stencils amplify
+    rounding by ~1e7, hence 1e-10 (1st derivative) and 1e-8 (2nd)."""
+    kat = json.loads((GOLD / "fd_coeff_kat.json").read_text())
+    n3 = kat["mesh"]["nP3"]
+    x3, _, _ = O.mesh_cosine(n3)
+    c = O.coeffs(x3)
+    pl = [x ** 3.0 - 5.0 * x ** 2.0 + 3.0 * x - 10.0 for x in x3]
+    got = {
+        "Bottom 1st Derivative": (c[0] * pl[0] + c[1] * pl[1]) + c[2] * pl[2],
+        "Top    1st Derivative": (c[6] * pl[-1] + c[7] * pl[-2]) + c[8] * pl[-3],
+        "Bottom 2nd Derivative": (c[3] * pl[0] + c[4] * pl[1]) + c[5] * pl[2],
+        "Top    2nd Derivative": (c[9] * pl[-1] + c[10] * pl[-2]) + c[11] * pl[-3],
+    }
+    for name, row in kat["rows"].items():
+        tol = 1e-10 if "1st" in name else 1e-8
+        assert abs(got[name] - row["logged"]) <= tol * abs(row["logged"]), (name, got[name], row)
+        # and the stencil is a derivative: exact value within its truncation error
+        assert abs(got[name] - row["exact"]) < 2e-3 * abs(row["exact"])
+
+
+def test_host_mesh_and_coeffs_match_oracle():
+    for n3 in (9, 65, 160):
+        x3, jac, inv = mesh_cosine(n3)
+        ox3, ojac, oinv = O.mesh_cosine(n3)
+        np.testing.assert_allclose(x3, ox3, rtol=0, atol=4e-16)
+        np.testing.assert_allclose(jac, ojac, rtol=1e-15, atol=1e-17)
+        c = wall_coeffs(ox3)
+        oc = O.coeffs(ox3)
+        names = ["f1d2c0", "f1d2c1", "f1d2c2", "f2d1c0", "f2d1c1", "f2d1c2",
+                 "b1d2c0", "b1d2c1", "b1d2c2", "b2d1c0", "b2d1c1", "b2d1c2", "dz1", "dzN"]
+        for i, n in enumerate(names):
+            assert c[n] == oc[i], n   # same formula, same operation order: bit-identical
+
+
+def test_coefficients_are_derivatives():
+    # one-sided 2nd-order first derivative is exact for quadratics; 2nd derivative for quadratics too
+    x3, _, _ = O.mesh_cosine(33)
+    c = O.coeffs(x3)
+    f = lambda x: 2.0 * x * x - 3.0 * x + 1.0
+    d1 = c[0] * f(x3[0]) + c[1] * f(x3[1]) + c[2] * f(x3[2])
+    d2 = c[3] * f(x3[0]) + c[4] * f(x3[1]) + c[5] * f(x3[2])
+    assert abs(d1 - (-3.0)) < 1e-9 and abs(d2 - 4.0) < 1e-6
+    b1 = c[6] * f(x3[-1]) + c[7] * f(x3[-2]) + c[8] * f(x3[-3])
+    assert abs(b1 - (4.0 * 2.0 - 3.0)) < 1e-9
+
+
+def _quiescent(p, x3):
+    n1, n2, n3 = p.nP
+    var = np.zeros((7, n3, n2, n1))
+    var[0] = 1.0
+    var[5] = 1.0
+    var[4] = 1.0
+    var[6] = 1.0 / (p.gama * p.Mac * p.Mac)
+    return var
+
+
+def test_quiescent_state_is_steady():
+    """u=v=w=0, rho=T=1, uniform p is an exact steady state of the scheme."""
+    from chan_cases import make_case
+    p, x3, jac, inv, _ = make_case(nP=(12, 10, 11), quantize=False, dt=1e-3)
+    var = _quiescent(p, x3)
+    o = O.Oracle(p, x3, jac, inv)
+    o.upload(var)
+    assert o.step(3) == 0
+    out = o.download()
+    np.testing.assert_allclose(out, var, rtol=0, atol=5e-14)
+
+
+def test_oracle_deterministic_and_thread_independent():
+    from chan_cases import make_case
+    p, x3, jac, inv, var = make_case(nP=(16, 10, 13), quantize=False)
+    outs = []
+    for th in (1, 3):
+        o = O.Oracle(p, x3, jac, inv, threads=th)
+        o.upload(var)
+        o.step(4)
+        outs.append(o.download())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_oracle_blowup_detection():
+    from chan_cases import make_case
+    p, x3, jac, inv, var = make_case(nP=(12, 10, 11), quantize=False)
+    var = var.copy()
+    var[0, 5, 4, 6] = -1.0   # negative density at one interior point
+    o = O.Oracle(p, x3, jac, inv)
+    o.upload(var)
+    assert o.step(5) == 1
+    f, ijk = o.blown()
+    assert f == 1 and o.nstep == 1
