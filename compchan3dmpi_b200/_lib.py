@@ -60,6 +60,7 @@ SIGNATURES = [
     ("chan_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("chan_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("chan_profile_read", ctypes.c_int, [ctypes.c_void_p, _D, _I64]),
+    ("chan_selftest_pow07", ctypes.c_int, [_D, _D, _D, ctypes.c_int64, ctypes.c_int32]),
     ("chan_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("chan_device_bytes", ctypes.c_int64, [ctypes.c_void_p]),
     ("chan_last_error", ctypes.c_char_p, [ctypes.c_void_p]),

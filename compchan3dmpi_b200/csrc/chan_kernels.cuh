@@ -182,6 +182,44 @@ __device__ __forceinline__ void visc_fy(const KParams &P, const Slot &s, const S
     g[3] = -((P.kq * mu) * Ty) + P.ggM * ((s.U[b] * g2 + s.V[b] * g3) + s.W[b] * g4);
 }
 
+// fD and gD together at one point: they share eight gradients, the shear
+// stress mu*(dv/dx+du/dy) (fD3 = gD2) and p + 2/3*mu*div.
+template <int BX>
+__device__ __forceinline__ void visc_fxy(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
+                                         const double *MU, const double *PR, int b, double czt, double f[4],
+                                         double g[4])
+{
+    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
+    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
+    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
+    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
+    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
+    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
+    const double Tx = (s.T[b + 1] - s.T[b - 1]) * P.hdx;
+    const double Ty = (s.T[b + BX] - s.T[b - BX]) * P.hdy;
+    const double uz = (sp.U[b] - sm.U[b]) * czt;
+    const double vz = (sp.V[b] - sm.V[b]) * czt;
+    const double wz = (sp.W[b] - sm.W[b]) * czt;
+    const double mu = MU[b], pr = PR[b];
+    const double u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
+    const double mr = mu * P.invRe, kqm = P.kq * mu;
+    const double div = (ux + vy) + wz;
+    const double pd = pr + (P.two3rd * mr) * div;
+    const double t12 = mr * (vx + uy);
+    const double f2 = pd - (2.0 * mr) * ux;
+    const double f4 = -(mr * (wx + uz));
+    const double g3 = pd - (2.0 * mr) * vy;
+    const double g4 = -(mr * (wy + vz));
+    f[0] = f2;
+    f[1] = -t12;
+    f[2] = f4;
+    f[3] = -(kqm * Tx) + P.ggM * ((u0 * f2 - v0 * t12) + w0 * f4);
+    g[0] = -t12;
+    g[1] = g3;
+    g[2] = g4;
+    g[3] = -(kqm * Ty) + P.ggM * ((-(u0 * t12) + v0 * g3) + w0 * g4);
+}
+
 // hD at the thread's own column; z-derivatives supplied by the caller
 template <int BX>
 __device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double mu, double pr, int b,
@@ -202,11 +240,44 @@ __device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double 
     h[3] = -((P.kq * mu) * Tz) + P.ggM * ((s.U[b] * h2 + s.V[b] * h3) + s.W[b] * h4);
 }
 
+// ---------------------------------------------------------------------------
+// Short math for the transport law mu = k = T^0.7 (main_v1.9.f90:643, 720) and
+// for 1/rho.  Both start from the single-precision hardware approximations
+// and refine in FP64.
+//
+// rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from a
+// float seed (relative error 2^-23 -> ~1e-14 -> ~1 ulp).  Valid for |x| in
+// the float normal range, which covers rho and mu of any physical state.
+__device__ __forceinline__ double rcp_fast(double x)
+{
+    double r = (double)__frcp_rn((float)x);
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+// pow07: y = T^0.7 is the positive root of y^10 = T^7.  One Halley step for
+// f(y) = y^10 - a, a = T^7:  y <- y * (9 y^10 + 11 a) / (11 y^10 + 9 a),
+// cubic convergence from a float seed exp2(0.7*log2 T) (relative error
+// ~3e-7 -> ~1e-19), so the result is limited by FP64 rounding (~2 ulp).
+// T <= 0 gives NaN, as the reference's T**0.7 would.
+__device__ __forceinline__ double pow07(double T)
+{
+    const float tf = (float)T;
+    double y = (double)exp2f(0.7f * __log2f(tf));
+    const double T2 = T * T, T4 = T2 * T2, a = (T4 * T2) * T;
+    const double y2 = y * y, y4 = y2 * y2, y8 = y4 * y4, u = y8 * y2;
+    const double num = fma(9.0, u, 11.0 * a);
+    const double den = fma(11.0, u, 9.0 * a);
+    return (y * num) * rcp_fast(den);
+}
+
 // primitives of one point from the conservative state (calcPrim, main_v1.9.f90:600-609)
 __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5], double &u, double &v,
                                              double &w, double &T)
 {
-    const double r = __drcp_rn(q[0]);
+    const double r = rcp_fast(q[0]);
     u = q[1] * r;
     v = q[2] * r;
     w = q[3] * r;
@@ -235,11 +306,16 @@ struct StageShape {
     static constexpr size_t bytes = sizeof(double) * (size_t)doubles;
 };
 
+#ifndef CHAN_MINB
+#define CHAN_MINB 2   // resident CTAs per SM the register budget is sized for
+#endif
+
 template <int TI, int TJ>
-__global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
+__global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 {
     using S = StageShape<TI, TJ>;
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT;
+    static_assert(2 * TJ <= 32 && 32 + 2 * TI <= NT, "halo-flux lane layout needs 2*TJ <= 32 and 32+2*TI <= TI*TJ");
     extern __shared__ double smem[];
     double *sPr = smem;            // [3][4][NB]
     double *sMP = sPr + 12 * NB;   // [2][2][NB]   mu, p
@@ -273,17 +349,35 @@ __global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
     auto spr = [&](int m) { return sMP + ((m & 1) * 2 + 1) * NB; };
     auto sq = [&](int m, int v) { return sQ + ((m & 1) * 5 + v) * NB; };
 
+    // box points this thread loads: the same columns for every plane
+    // lp: box index | 0x10000 if the point is in R1 (tile plus a 1-point cross
+    // halo, where mu is needed); -1 if outside the array.  lo: column offset.
+    constexpr int NL = (NB + NT - 1) / NT;
+    int lp[NL];
+    int lo[NL];
+#pragma unroll
+    for (int l = 0; l < NL; l++) {
+        const int p = tid + l * NT;
+        const int bj = p / BX, bi = p - bj * BX;
+        const int gi = i0 - 2 + bi, gj = j0 - 2 + bj;
+        const bool ok = p < NB && gi <= n1 + 1 && gj <= n2 + 1;
+        const bool r1 = (bi >= 1 && bi <= BX - 2 && bj >= 2 && bj <= BY - 3) ||
+                        (bi >= 2 && bi <= BX - 3 && bj >= 1 && bj <= BY - 2);
+        lp[l] = ok ? (p | (r1 ? 0x10000 : 0)) : -1;
+        lo[l] = gj * P.px + gi;
+    }
+
     // fill the ring slots of plane m over the whole box
     auto load_plane = [&](int m) {
         const Slot s = slot(m);
         double *MU = smu(m), *PR = spr(m);
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
-        for (int p = tid; p < NB; p += NT) {
-            const int bj = p / BX, bi = p - bj * BX;
-            const int gi = i0 - 2 + bi, gj = j0 - 2 + bj;
-            if (gi > n1 + 1 || gj > n2 + 1) continue;
-            const long long off = (long long)m * plane + (long long)gj * P.px + gi;
+#pragma unroll
+        for (int l = 0; l < NL; l++) {
+            if (lp[l] < 0) continue;
+            const int p = lp[l] & 0xffff;
+            const long long off = (long long)m * plane + lo[l];
             double q[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
@@ -292,7 +386,7 @@ __global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
             }
             double u, vv, w, T, mu, pr;
             if (wall) {
-                const long long wo = (long long)gj * P.px + gi;
+                const long long wo = lo[l];
                 u = W[1 * plane + wo];
                 vv = W[2 * plane + wo];
                 w = W[3 * plane + wo];
@@ -302,9 +396,7 @@ __global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
             } else {
                 prims_from_q(P, q, u, vv, w, T);
                 pr = (q[0] * T) * P.inv_gM2;
-                const bool r1 = (bi >= 1 && bi <= BX - 2 && bj >= 2 && bj <= BY - 3) ||
-                                (bi >= 2 && bi <= BX - 3 && bj >= 1 && bj <= BY - 2);
-                mu = r1 ? pow(T, 0.7) : 0.0;
+                mu = (lp[l] & 0x10000) ? pow07(T) : 0.0;
             }
             ((double *)s.U)[p] = u;
             ((double *)s.V)[p] = vv;
@@ -392,39 +484,43 @@ __global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
         // ---------- C: viscous flux vectors
         const Slot s0 = slot(t), sm = slot(t - 1), sp = slot(t + 1);
         double hp1[4] = {0, 0, 0, 0};
-        if (col_ok) {
-            if (t + 1 == n3)
-                hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], sp.U[bc], sp.V[bc], sp.W[bc], sp.T[bc], hp1);
-            else
-                hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+        // RK base state of the own point, fetched early (stages that use it)
+        {
             const double czt = P.czh[t];
             const double *MU = smu(t), *PR = spr(t);
-            double f[4];
-            visc_fx<BX>(P, s0, sm, sp, MU, PR, bc, czt, f);
+            if (col_ok) {
+                if (t + 1 == n3)
+                    hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], sp.U[bc], sp.V[bc], sp.W[bc], sp.T[bc], hp1);
+                else
+                    hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+                double f[4], g[4];
+                visc_fxy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f, g);
 #pragma unroll
-            for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
-            if (tx == 0) {
-                visc_fx<BX>(P, s0, sm, sp, MU, PR, bc - 1, czt, f);
-#pragma unroll
-                for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + 0] = f[c];
+                for (int c = 0; c < 4; c++) {
+                    sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
+                    sG[(c * (TJ + 2) + ty + 1) * TI + tx] = g[c];
+                }
             }
-            if (tx == TI - 1 && i + 1 <= n1) {
-                visc_fx<BX>(P, s0, sm, sp, MU, PR, bc + 1, czt, f);
+            // halo fluxes on dedicated lanes: fD of the two x-halo columns on
+            // lanes 0..2TJ-1 of warp 0, gD of the two y-halo rows on warps 1..
+            if (tid < 2 * TJ) {
+                const int side = tid / TJ, r = tid - side * TJ;
+                const int ci = side ? i0 + TI : i0 - 1, cj = j0 + r;
+                if (ci <= n1 && cj <= n2) {
+                    double f[4];
+                    visc_fx<BX>(P, s0, sm, sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1), czt, f);
 #pragma unroll
-                for (int c = 0; c < 4; c++) sF[(c * TJ + ty) * (TI + 2) + TI + 1] = f[c];
-            }
-            visc_fy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f);
+                    for (int c = 0; c < 4; c++) sF[(c * TJ + r) * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
+                }
+            } else if (tid >= 32 && tid < 32 + 2 * TI) {
+                const int h = tid - 32, side = h / TI, cc = h - side * TI;
+                const int ci = i0 + cc, cj = side ? j0 + TJ : j0 - 1;
+                if (ci <= n1 && cj <= n2) {
+                    double g[4];
+                    visc_fy<BX>(P, s0, sm, sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2, czt, g);
 #pragma unroll
-            for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + ty + 1) * TI + tx] = f[c];
-            if (ty == 0) {
-                visc_fy<BX>(P, s0, sm, sp, MU, PR, bc - BX, czt, f);
-#pragma unroll
-                for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + 0) * TI + tx] = f[c];
-            }
-            if (ty == TJ - 1 && j + 1 <= n2) {
-                visc_fy<BX>(P, s0, sm, sp, MU, PR, bc + BX, czt, f);
-#pragma unroll
-                for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + TJ + 1) * TI + tx] = f[c];
+                    for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + (side ? TJ + 1 : 0)) * TI + cc] = g[c];
+                }
             }
         }
         __syncthreads();
@@ -512,17 +608,21 @@ __global__ void __launch_bounds__(TI *TJ, 2) k_stage(const KParams P)
             R[4] = src5 - R[4];
             // RK update
             double qn[5];
-            const long long off = (long long)t * plane + colo;
+            double qb[5] = {0, 0, 0, 0, 0};
+            if (P.rk_mode != 0) {
+                const long long off = (long long)t * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) qb[c] = __ldg(P.qbase + c * vol + off);
+            }
             if (P.rk_mode == 0) {
 #pragma unroll
                 for (int c = 0; c < 5; c++) qn[c] = q0[c] + P.rk_cdt * R[c];
             } else if (P.rk_mode == 1) {
 #pragma unroll
-                for (int c = 0; c < 5; c++) qn[c] = __ldg(P.qbase + c * vol + off) + P.rk_cdt * R[c];
+                for (int c = 0; c < 5; c++) qn[c] = qb[c] + P.rk_cdt * R[c];
             } else {
 #pragma unroll
-                for (int c = 0; c < 5; c++)
-                    qn[c] = (P.rk_a * __ldg(P.qbase + c * vol + off) + P.rk_b * q0[c]) + P.rk_cdt * R[c];
+                for (int c = 0; c < 5; c++) qn[c] = (P.rk_a * qb[c] + P.rk_b * q0[c]) + P.rk_cdt * R[c];
             }
             // store + periodic images (the ghosts the reference's halo exchange fills)
             const int im = (i <= 3) ? i + (n1 - 2) : ((i >= n1 - 2) ? i - (n1 - 2) : -1);
@@ -868,6 +968,15 @@ __global__ void k_check(const KParams P, const double *q)
         double x[7];
         ref_var(P, q, ii + 1, jj + 1, kk + 1, x);
         if (x[0] < 0.0 || x[5] < 0.0) flag_blown(P.status, ii + 1, jj + 1, kk + 1, P.step);
+    }
+}
+
+// self-test of pow07 against the CUDA math library's pow (diagnostics only)
+__global__ void k_selftest_pow07(const double *T, double *mine, double *libm, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        mine[i] = pow07(T[i]);
+        libm[i] = pow(T[i], 0.7);
     }
 }
 

@@ -14,8 +14,15 @@
 
 namespace {
 
-constexpr int TI = 32;  // stage-kernel tile: 32 columns in x (one warp row)
-constexpr int TJ = 8;   // 8 rows in y -> 256 threads, 2 CTAs per SM
+// stage-kernel tile: TI columns in x (one warp row) by TJ rows in y
+#ifndef CHAN_TI
+#define CHAN_TI 32
+#endif
+#ifndef CHAN_TJ
+#define CHAN_TJ 8
+#endif
+constexpr int TI = CHAN_TI;
+constexpr int TJ = CHAN_TJ;
 
 std::string g_init_error;
 
@@ -561,6 +568,25 @@ int chan_profile_read(chan_ctx *c, double *ms3, int64_t *count3)
 }
 
 void *chan_stream(chan_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int chan_selftest_pow07(const double *T, double *mine, double *libm, int64_t n, int32_t device)
+{
+    if (!T || !mine || !libm || n <= 0) return CHAN_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return CHAN_ECUDA;
+    double *d = nullptr;
+    const size_t b = (size_t)n * sizeof(double);
+    if (cudaMalloc((void **)&d, 3 * b) != cudaSuccess) return CHAN_ENOMEM;
+    cudaError_t e = cudaMemcpy(d, T, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        chan::k_selftest_pow07<<<256, 256>>>(d, d + n, d + 2 * n, (long long)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(mine, d + n, b, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(libm, d + 2 * n, b, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { g_init_error = cudaGetErrorString(e); return CHAN_ECUDA; }
+    return CHAN_OK;
+}
 
 int64_t chan_device_bytes(chan_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
 

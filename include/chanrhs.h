@@ -141,6 +141,12 @@ int chan_sync(chan_ctx *c);
 int chan_profile(chan_ctx *c, int enable);
 int chan_profile_read(chan_ctx *c, double *ms3, int64_t *count3);
 
+/* Diagnostics: evaluate the library's T^0.7 (the transport law mu = k = T^0.7
+ * of main_v1.9.f90:643,720) and the CUDA math library's pow(T,0.7) on device
+ * `device` for n host values; results go to host arrays mine and libm.
+ * The reference has no counterpart. */
+int chan_selftest_pow07(const double *T, double *mine, double *libm, int64_t n, int32_t device);
+
 /* The context's cudaStream_t (as void*), for callers that record events. */
 void *chan_stream(chan_ctx *c);
 
