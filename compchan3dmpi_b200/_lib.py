@@ -65,6 +65,7 @@ SIGNATURES = [
     ("chan_device_bytes", ctypes.c_int64, [ctypes.c_void_p]),
     ("chan_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("chan_version", ctypes.c_char_p, []),
+    ("chan_avg_spatial_noalloc", ctypes.c_int, [_D, _I32, _D, _D, _D, ctypes.c_int32]),
     ("chan_free", None, [ctypes.c_void_p]),
 ]
 

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -252,6 +253,83 @@ int dalloc(chan_ctx *c, double **p, size_t n)
     e = cudaMemsetAsync(*p, 0, n * sizeof(double), c->stream);
     if (e != cudaSuccess) return fail(c, "cudaMemsetAsync", e);
     return CHAN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free plane moments.
+//
+// Fortran post-processing programs of the reference (avg_v1.7.f90, fluc.f90)
+// bind through iso_c_binding and have no way to call cudaMalloc or to keep a
+// solver context, so they cannot supply device buffers.  chan_avg_spatial_noalloc
+// serves them from one file-scope device array of fixed size.  Every GPU that
+// loads this library holds the array until the process exits.
+//
+// Layout of the array per call: [23*nP3 results][7*nk*nP1*nP2 staged slab].
+// Calls share the array and it keeps the last call's contents; calls that
+// overlap on the GPU (two host threads, or two streams) race on it.
+static __device__ __align__(256) double g_noalloc_scratch[CHAN_NOALLOC_MAX_DOUBLES];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[256] = {nullptr};  // device address of the array, per device
+
+// device address of g_noalloc_scratch on the current device; resolved once per device
+double *noalloc_scratch(int dev)
+{
+    if (dev < 0 || dev >= 256) return nullptr;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            g_init_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        g_noalloc_addr[dev] = (double *)p;
+    }
+    return g_noalloc_addr[dev];
+}
+
+// plane moments of a staged slab of var planes k0..k0+nk-1; same per-plane
+// reduction order as k_stats
+__global__ void __launch_bounds__(chan::kStatThreads) k_moments_slab(const double *slab, int n1, int n2, int nk,
+                                                                     int k0, int n3, double *res)
+{
+    __shared__ double red[chan::kStatThreads / 32][23];
+    const int kk = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long pl = (long long)n1 * n2;
+    double acc[23];
+#pragma unroll
+    for (int c = 0; c < 23; c++) acc[c] = 0.0;
+    for (long long p = tid; p < pl; p += chan::kStatThreads) {
+        double x[7];
+#pragma unroll
+        for (int m = 0; m < 7; m++) x[m] = slab[((long long)m * nk + kk) * pl + p];
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+            acc[m] += x[m];
+            acc[7 + m] += x[m] * x[m];
+        }
+        acc[14] += x[0] * x[3];
+        acc[15] += x[0] * x[5];
+        acc[16] += x[1] * x[2];
+        acc[17] += x[1] * x[3];
+        acc[18] += x[2] * x[3];
+        acc[19] += x[2] * x[5];
+        acc[20] += x[5] * x[3];
+        acc[21] += x[6] * x[3];
+        acc[22] += x[6] * x[5];
+    }
+#pragma unroll
+    for (int c = 0; c < 23; c++) {
+        const double sum = chan::warp_sum(acc[c]);
+        if (lane == 0) red[warp][c] = sum;
+    }
+    __syncthreads();
+    if (tid < 23) {
+        double sum = 0.0;
+        for (int w = 0; w < chan::kStatThreads / 32; w++) sum += red[w][tid];
+        res[(long long)tid * n3 + k0 + kk] = sum / (double)(n1 * n2);
+    }
 }
 
 }  // namespace
@@ -589,6 +667,56 @@ int chan_selftest_pow07(const double *T, double *mine, double *libm, int64_t n, 
 }
 
 int64_t chan_device_bytes(chan_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
+
+int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1, double *stat2, double *corr,
+                             int32_t device)
+{
+    g_init_error.clear();
+    if (!var || !nP || !stat1 || !stat2 || !corr) { g_init_error = "NULL argument"; return CHAN_EINVAL; }
+    const int n1 = nP[0], n2 = nP[1], n3 = nP[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1) { g_init_error = "every nP must be >= 1"; return CHAN_EINVAL; }
+    const long long pl = (long long)n1 * n2;
+    const long long head = (23LL * n3 + 31) / 32 * 32;
+    if (head + 7 * pl > (long long)CHAN_NOALLOC_MAX_DOUBLES) {
+        char buf[256];
+        snprintf(buf, sizeof(buf),
+                 "chan_avg_spatial_noalloc: 23*nP3 + 7*nP1*nP2 = %lld doubles exceeds the fixed area of %d doubles",
+                 head + 7 * pl, (int)CHAN_NOALLOC_MAX_DOUBLES);
+        g_init_error = buf;
+        return CHAN_EINVAL;
+    }
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { g_init_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return CHAN_ECUDA; }
+    double *scr = noalloc_scratch(device);
+    if (!scr) { cudaSetDevice(prev); return CHAN_ECUDA; }
+    double *res = scr, *slab = scr + head;
+    const long long kslab_ll = ((long long)CHAN_NOALLOC_MAX_DOUBLES - head) / (7 * pl);
+    const int kslab = (int)(kslab_ll < n3 ? kslab_ll : n3);
+    // the results must start at zero: every plane is written below, and a
+    // failed call must not hand back the previous call's numbers
+    e = cudaMemsetAsync(res, 0, 23 * (size_t)n3 * sizeof(double), 0);
+    for (int k0 = 0; k0 < n3 && e == cudaSuccess; k0 += kslab) {
+        const int nk = (n3 - k0) < kslab ? (n3 - k0) : kslab;
+        for (int m = 0; m < 7 && e == cudaSuccess; m++)
+            e = cudaMemcpyAsync(slab + (size_t)m * nk * pl, var + ((size_t)m * n3 + k0) * pl,
+                                (size_t)nk * pl * sizeof(double), cudaMemcpyHostToDevice, 0);
+        if (e == cudaSuccess) {
+            k_moments_slab<<<nk, chan::kStatThreads, 0, 0>>>(slab, n1, n2, nk, k0, n3, res);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stat1, res, 7 * (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(stat2, res + 7 * (size_t)n3, 7 * (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(corr, res + 14 * (size_t)n3, 9 * (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) { g_init_error = std::string("chan_avg_spatial_noalloc: ") + cudaGetErrorString(e); return CHAN_ECUDA; }
+    return CHAN_OK;
+}
 
 void chan_free(chan_ctx *c)
 {

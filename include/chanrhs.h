@@ -159,6 +159,36 @@ const char *chan_last_error(chan_ctx *c);
 /* Library version string. */
 const char *chan_version(void);
 
+/* Plane moments stat1Spc, stat2Spc, corrSpc of a host field, computed on GPU
+ * `device` without allocating any memory.  This entry point has no
+ * counterpart in the reference.
+ *
+ * Who needs it: Fortran post-processing programs like the reference's
+ * avg_v1.7.f90 and fluc.f90 call through iso_c_binding and have no way to
+ * call cudaMalloc or to keep a solver context (chan_init allocates the whole
+ * solver state).  This call needs neither.  It stages the field through one
+ * static device array of CHAN_NOALLOC_MAX_DOUBLES doubles (32 MiB), which
+ * every GPU that loads the library holds until the process exits.
+ * The results equal chan_avg_spatial + chan_stats on the same field
+ * (v1.9/codes/main_v1.9.f90:995-1025 semantics: sums over i=1..nP1,
+ * j=1..nP2 divided by nP1*nP2).
+ *
+ * var    : var(1:nP1,1:nP2,1:nP3,1:7) in host memory.
+ * nP     : nP1, nP2, nP3.
+ * stat1, stat2 : 7*nP3 doubles each, stored [p][k];  corr : 9*nP3, [c][k].
+ * Limit  : 23*nP3 (rounded up to 32) + 7*nP1*nP2 <= CHAN_NOALLOC_MAX_DOUBLES,
+ *          i.e. one full wall-normal plane of all seven variables must fit;
+ *          larger grids return CHAN_EINVAL with a message (chan_last_error(NULL)).
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress, no allocation); make that first call before any
+ * stream capture.  It works on the legacy default stream and synchronizes
+ * it.  It restores the calling thread's current device on return.
+ * All calls share the one array: calls that overlap on the GPU (concurrent
+ * host threads on the same device) race and must be serialized by the caller. */
+#define CHAN_NOALLOC_MAX_DOUBLES (4 * 1024 * 1024)
+int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1, double *stat2, double *corr,
+                             int32_t device);
+
 /* Free device memory and the context.  NULL is allowed. */
 void chan_free(chan_ctx *c);
 
