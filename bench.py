@@ -126,17 +126,18 @@ def hbm_peak():
 
 
 def measured_traffic(p, n_int):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
-    f = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    """Per-launch DRAM bytes of the stage kernel: the per-point figure of the
+    committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum over
+    one RK3 step of a 4.6 M-point case) scaled by this workload's points."""
+    f = os.path.join(ROOT, "profiles", "stage_kernel_256x192x97_full.md")
     try:
         with open(f) as fh:
-            d = json.load(fh)
+            for ln in fh:
+                if ln.startswith("traffic_bytes_per_updated_point_per_launch"):
+                    return float(ln.split("=")[1]) * n_int
     except (OSError, ValueError):
         return None
-    bpp = d.get("dram_bytes_per_updated_point_per_stage")
-    if bpp is None:
-        return None
-    return float(bpp) * n_int
+    return None
 
 
 # --------------------------------------------------------------- CPU
