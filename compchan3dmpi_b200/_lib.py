@@ -15,7 +15,7 @@ LIBDIR = HERE / "lib"
 LIBNAME = "libchanrhs.so"
 
 CHAN_OK, CHAN_BLOWUP, CHAN_NONFINITE = 0, 1, 2
-CHAN_EINVAL, CHAN_ENOMEM, CHAN_ECUDA, CHAN_ESTATE = -1, -2, -3, -4
+CHAN_EINVAL, CHAN_ENOMEM, CHAN_ECUDA, CHAN_ESTATE, CHAN_EIO = -1, -2, -3, -4, -5
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I32 = ctypes.POINTER(ctypes.c_int32)
@@ -65,6 +65,14 @@ SIGNATURES = [
     ("chan_device_bytes", ctypes.c_int64, [ctypes.c_void_p]),
     ("chan_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("chan_version", ctypes.c_char_p, []),
+    ("chan_time_avg_start", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_time_avg", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _I64, _D, _D]),
+    ("chan_checkpoint_write", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("chan_checkpoint_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("chan_deck_read", ctypes.c_int, [ctypes.c_char_p, _I32, _D, _D, _D, _D, _D, _I64, ctypes.c_int32]),
+    ("chan_deck_write", ctypes.c_int, [ctypes.c_char_p, _I32, _D, _D, _D, _D, ctypes.c_double, ctypes.c_int64,
+                                       ctypes.c_int32]),
+    ("chan_io_last_error", ctypes.c_char_p, []),
     ("chan_avg_spatial_noalloc", ctypes.c_int, [_D, _I32, _D, _D, _D, ctypes.c_int32]),
     ("chan_free", None, [ctypes.c_void_p]),
 ]

@@ -19,15 +19,17 @@ OUT = HERE / "lib" / "libchanrhs.so"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", f"-I{ROOT / 'include'}"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread", "-shared",
+         f"-I{ROOT / 'include'}"]
 
 
 def sources():
-    return [SRC / "chanrhs.cu"]
+    return [SRC / "chanrhs.cu", SRC / "deck_io.cpp"]
 
 
 def deps():
-    return sorted(SRC.glob("*.cu")) + sorted(SRC.glob("*.cuh")) + [ROOT / "include" / "chanrhs.h"]
+    return sorted(SRC.glob("*.cu")) + sorted(SRC.glob("*.cuh")) + sorted(SRC.glob("*.cpp")) + \
+        [ROOT / "include" / "chanrhs.h"]
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:

@@ -114,10 +114,17 @@ class Channel:
         self._check(self.L.chan_upload(self._h, _lib.dptr(v), int(nstep), float(time)))
 
     def read_input_file(self, path):
-        from .deck import read_3d_dat
-        var, time, nstep, *_ = read_3d_dat(path, self.nP)
+        from .deck import read_3d_dat_native
+        var, time, nstep, *_ = read_3d_dat_native(path, self.nP)
         self.init_sol_v(var, nstep, time)
         return var
+
+    def checkpoint_write(self, path):
+        """Exact binary checkpoint of the device state (between steps)."""
+        self._check(self.L.chan_checkpoint_write(self._h, str(path).encode()))
+
+    def checkpoint_read(self, path):
+        self._check(self.L.chan_checkpoint_read(self._h, str(path).encode()))
 
     def stage(self, it: int):
         return self._check(self.L.chan_stage(self._h, int(it)))
@@ -146,6 +153,23 @@ class Channel:
         self._check(self.L.chan_stats(self._h, _lib.dptr(tau), _lib.dptr(s1), _lib.dptr(s2), _lib.dptr(c)))
         return tau, s1, s2, c
 
+    def time_avg_start(self):
+        """Start device-side time averaging of the statistics steps."""
+        self._check(self.L.chan_time_avg_start(self._h))
+
+    def time_average(self):
+        """avg_v1.7.f90 over the statistics steps since time_avg_start:
+        dict with mean, rms, covar, tau (means), samples, t0, t1."""
+        from .stats import time_average
+        n3 = self.nP[2]
+        s1 = np.zeros((7, n3)); s2 = np.zeros((7, n3)); sc = np.zeros((9, n3)); st = np.zeros(2)
+        n = ctypes.c_int64(); t0 = ctypes.c_double(); t1 = ctypes.c_double()
+        self._check(self.L.chan_time_avg(self._h, _lib.dptr(s1), _lib.dptr(s2), _lib.dptr(sc), _lib.dptr(st),
+                                         ctypes.byref(n), ctypes.byref(t0), ctypes.byref(t1)))
+        mean, rms, covar, tau = time_average(s1, s2, sc, st, n.value)
+        return {"mean": mean, "rms": rms, "covar": covar, "tau": tau, "samples": n.value,
+                "t0": t0.value, "t1": t1.value}
+
     def set_forcing(self, tauL: float, tauU: float, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         self._check(self.L.chan_set_forcing(self._h, float(tauL), float(tauU), _lib.dptr(rb)))
@@ -158,12 +182,12 @@ class Channel:
         return out
 
     def write_soln(self, path):
-        from .deck import write_3d_dat
+        from .deck import write_3d_dat_native
         from .mesh import periodic_coords
         var = self.download()
         _, n, t = self.status_detail()
-        write_3d_dat(path, var, periodic_coords(self.nP[0], self.params.Lx),
-                     periodic_coords(self.nP[1], self.params.Ly), self.x3, t, n)
+        write_3d_dat_native(path, var, periodic_coords(self.nP[0], self.params.Lx),
+                            periodic_coords(self.nP[1], self.params.Ly), self.x3, t, n)
 
     def status_detail(self):
         ijk = (ctypes.c_int32 * 3)()

@@ -48,6 +48,7 @@ struct KParams {
     const double *pez;    // Re*dXi*jac(k)
     // forcing / stats
     double *stat;         // stat1[7*n3] | stat2[7*n3] | corr[9*n3] | tau[2]
+    double *tacc;         // running sums of the same 23*n3+2 numbers over statistics steps
     DevStatus *status;
     // physics
     double invRe, ggM, ggMh, gM2, inv_gM2, kq, two3rd;
@@ -62,6 +63,7 @@ struct KParams {
     int rk_mode;          // 0: in + cdt*R ; 1: base + cdt*R ; 2: a*base + b*in + cdt*R
     int check;            // last stage of a step: run the blow-up test
     int force_on;
+    int acc_on;           // statistics steps also add into tacc (time averaging)
     long long step;       // step number being computed
 };
 
@@ -825,7 +827,9 @@ __global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const d
             if (tid < 7) out = P.stat + (size_t)tid * n3;
             else if (tid < 14) out = P.stat + (size_t)7 * n3 + (size_t)(tid - 7) * n3;
             else out = P.stat + (size_t)14 * n3 + (size_t)(tid - 14) * n3;
-            out[k - 1] = s / nxy;
+            const double val = s / nxy;
+            out[k - 1] = val;
+            if (P.acc_on) P.tacc[(out - P.stat) + (k - 1)] += val;
         }
         return;
     }
@@ -853,7 +857,9 @@ __global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const d
     if (tid == 0) {
         double t = 0.0;
         for (int w = 0; w < kStatThreads / 32; w++) t += red[w][0];
-        P.stat[(size_t)23 * n3 + wall] = t / (double)np;
+        const double val = t / (double)np;
+        P.stat[(size_t)23 * n3 + wall] = val;
+        if (P.acc_on) P.tacc[(size_t)23 * n3 + wall] += val;
     }
 }
 

@@ -40,7 +40,9 @@ struct chan_ctx {
     cudaStream_t stream = nullptr;
     chan::KParams kp{};
     double *q[3] = {nullptr, nullptr, nullptr};
-    double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr;
+    double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr, *tacc = nullptr;
+    long long tavg_samples = 0;  // statistics steps summed into tacc since chan_time_avg_start
+    double tavg_t0 = 0.0, tavg_t1 = 0.0;
     chan::DevStatus *status = nullptr;
     chan::DevStatus *h_status = nullptr;
     int n1 = 0, n2 = 0, n3 = 0, px = 0, NJ = 0;
@@ -205,12 +207,17 @@ int enqueue_steps(chan_ctx *c, int nsteps)
             int r = launch_stage(c, it, it == c->nstage, step);
             if (r) return r;
         }
+        c->nstep = step;
+        c->time = c->time + c->p.dt;
         if (c->p.istat > 0 && step % c->p.istat == 0) {
             int r = launch_stats(c, step, 1, 1);
             if (r) return r;
+            if (c->kp.acc_on) {
+                if (c->tavg_samples == 0) c->tavg_t0 = c->time;
+                c->tavg_t1 = c->time;
+                c->tavg_samples++;
+            }
         }
-        c->nstep = step;
-        c->time = c->time + c->p.dt;
     }
     return CHAN_OK;
 }
@@ -384,6 +391,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
         if ((r = dalloc(c, &c->q[b], 5 * (size_t)c->vol))) { g_init_error = c->err; chan_free(c); return r; }
     if ((r = dalloc(c, &c->wp, 2 * 8 * (size_t)c->plane)) || (r = dalloc(c, &c->cs, (size_t)(n3 + 2) * 28)) ||
         (r = dalloc(c, &c->tabs, 4 * (size_t)(n3 + 2))) || (r = dalloc(c, &c->stat, 23 * (size_t)n3 + 2)) ||
+        (r = dalloc(c, &c->tacc, 23 * (size_t)n3 + 2)) ||
         (r = dalloc(c, &c->dvar, 7 * (size_t)n1 * n2 * n3))) {
         g_init_error = c->err;
         chan_free(c);
@@ -418,7 +426,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     k.plane = c->plane; k.vol = c->vol;
     k.wp = c->wp; k.cs = c->cs;
     k.czh = c->tabs; k.cz8 = c->tabs + (n3 + 2); k.cz12 = c->tabs + 2 * (n3 + 2); k.pez = c->tabs + 3 * (n3 + 2);
-    k.stat = c->stat; k.status = c->status;
+    k.stat = c->stat; k.status = c->status; k.tacc = c->tacc; k.acc_on = 0;
     k.invRe = 1.0 / Re;
     k.ggM = gama * (gama - 1) * (Mac * Mac);
     k.ggMh = k.ggM * 0.5;
@@ -668,6 +676,124 @@ int chan_selftest_pow07(const double *T, double *mine, double *libm, int64_t n, 
 
 int64_t chan_device_bytes(chan_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
 
+// ---------------------------------------------------------------------------
+// Exact checkpoint of the device state: the conservative state with its
+// ghosts, the wall planes, the stale corner columns, the forcing/statistics
+// state and the counters, in native byte order.
+namespace {
+const char kCkpMagic[8] = {'C', 'H', 'A', 'N', 'C', 'K', 'P', '1'};
+struct CkpHeader {
+    char magic[8];
+    int32_t nP[3];
+    int32_t px;
+    int64_t nstep;
+    double time;
+    int64_t tavg_samples;
+    double tavg_t0, tavg_t1;
+    int32_t acc_on;
+    int32_t pad;
+};
+}  // namespace
+
+int chan_checkpoint_write(chan_ctx *c, const char *path)
+{
+    if (!c || !path) return CHAN_EINVAL;
+    if (!c->uploaded) { c->err = "checkpoint before chan_upload"; return CHAN_ESTATE; }
+    if (c->cur != 0) { c->err = "checkpoint only between time steps"; return CHAN_ESTATE; }
+    int r = read_status(c, nullptr);
+    if (r == CHAN_BLOWUP) { c->err = "state blew up; no checkpoint"; return CHAN_ESTATE; }
+    CK(c, cudaSetDevice(c->dev));
+    CkpHeader h{};
+    memcpy(h.magic, kCkpMagic, 8);
+    for (int m = 0; m < 3; m++) h.nP[m] = c->p.nP[m];
+    h.px = c->px; h.nstep = c->nstep; h.time = c->time;
+    h.tavg_samples = c->tavg_samples; h.tavg_t0 = c->tavg_t0; h.tavg_t1 = c->tavg_t1; h.acc_on = c->kp.acc_on;
+    const size_t nq = 5 * (size_t)c->vol, nw = 16 * (size_t)c->plane, ncs = (size_t)(c->n3 + 2) * 28,
+                 nst = 23 * (size_t)c->n3 + 2;
+    std::vector<double> hb(nq + nw + ncs + 2 * nst);
+    double *o = hb.data();
+    CK(c, cudaMemcpyAsync(o, c->q[0], nq * sizeof(double), cudaMemcpyDeviceToHost, c->stream)); o += nq;
+    CK(c, cudaMemcpyAsync(o, c->wp, nw * sizeof(double), cudaMemcpyDeviceToHost, c->stream)); o += nw;
+    CK(c, cudaMemcpyAsync(o, c->cs, ncs * sizeof(double), cudaMemcpyDeviceToHost, c->stream)); o += ncs;
+    CK(c, cudaMemcpyAsync(o, c->stat, nst * sizeof(double), cudaMemcpyDeviceToHost, c->stream)); o += nst;
+    CK(c, cudaMemcpyAsync(o, c->tacc, nst * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    FILE *f = fopen(path, "wb");
+    if (!f) { c->err = std::string("cannot open ") + path; return CHAN_EIO; }
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(hb.data(), sizeof(double), hb.size(), f) == hb.size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) { c->err = std::string("write failed: ") + path; return CHAN_EIO; }
+    return CHAN_OK;
+}
+
+int chan_checkpoint_read(chan_ctx *c, const char *path)
+{
+    if (!c || !path) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    FILE *f = fopen(path, "rb");
+    if (!f) { c->err = std::string("cannot open ") + path; return CHAN_EIO; }
+    CkpHeader h{};
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, kCkpMagic, 8) != 0) {
+        fclose(f);
+        c->err = std::string("not a checkpoint of this library: ") + path;
+        return CHAN_EIO;
+    }
+    if (h.nP[0] != c->p.nP[0] || h.nP[1] != c->p.nP[1] || h.nP[2] != c->p.nP[2] || h.px != c->px) {
+        fclose(f);
+        c->err = "checkpoint grid differs from the context's";
+        return CHAN_EINVAL;
+    }
+    const size_t nq = 5 * (size_t)c->vol, nw = 16 * (size_t)c->plane, ncs = (size_t)(c->n3 + 2) * 28,
+                 nst = 23 * (size_t)c->n3 + 2;
+    std::vector<double> hb(nq + nw + ncs + 2 * nst);
+    const bool ok = fread(hb.data(), sizeof(double), hb.size(), f) == hb.size();
+    fclose(f);
+    if (!ok) { c->err = std::string("checkpoint truncated: ") + path; return CHAN_EIO; }
+    const double *o = hb.data();
+    for (int b = 0; b < 3; b++)
+        CK(c, cudaMemcpyAsync(c->q[b], o, nq * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    o += nq;
+    CK(c, cudaMemcpyAsync(c->wp, o, nw * sizeof(double), cudaMemcpyHostToDevice, c->stream)); o += nw;
+    CK(c, cudaMemcpyAsync(c->cs, o, ncs * sizeof(double), cudaMemcpyHostToDevice, c->stream)); o += ncs;
+    CK(c, cudaMemcpyAsync(c->stat, o, nst * sizeof(double), cudaMemcpyHostToDevice, c->stream)); o += nst;
+    CK(c, cudaMemcpyAsync(c->tacc, o, nst * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(c->status, 0, sizeof(chan::DevStatus), c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->nstep = h.nstep; c->time = h.time; c->sync_nstep = h.nstep; c->sync_time = h.time;
+    c->tavg_samples = h.tavg_samples; c->tavg_t0 = h.tavg_t0; c->tavg_t1 = h.tavg_t1; c->kp.acc_on = h.acc_on;
+    c->cur = 0;
+    c->uploaded = true;
+    return CHAN_OK;
+}
+
+int chan_time_avg_start(chan_ctx *c)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    CK(c, cudaMemsetAsync(c->tacc, 0, (23 * (size_t)c->n3 + 2) * sizeof(double), c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->tavg_samples = 0;
+    c->kp.acc_on = 1;
+    return CHAN_OK;
+}
+
+int chan_time_avg(chan_ctx *c, double *sum1, double *sum2, double *sumc, double *sumtau, int64_t *nsamples,
+                  double *t0, double *t1)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t n3 = (size_t)c->n3;
+    if (sum1) CK(c, cudaMemcpyAsync(sum1, c->tacc, 7 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (sum2) CK(c, cudaMemcpyAsync(sum2, c->tacc + 7 * n3, 7 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (sumc) CK(c, cudaMemcpyAsync(sumc, c->tacc + 14 * n3, 9 * n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (sumtau) CK(c, cudaMemcpyAsync(sumtau, c->tacc + 23 * n3, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (nsamples) *nsamples = c->tavg_samples;
+    if (t0) *t0 = c->tavg_t0;
+    if (t1) *t1 = c->tavg_t1;
+    return CHAN_OK;
+}
+
 int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1, double *stat2, double *corr,
                              int32_t device)
 {
@@ -729,6 +855,7 @@ void chan_free(chan_ctx *c)
     if (c->wp) cudaFree(c->wp);
     if (c->cs) cudaFree(c->cs);
     if (c->tabs) cudaFree(c->tabs);
+    if (c->tacc) cudaFree(c->tacc);
     if (c->stat) cudaFree(c->stat);
     if (c->dvar) cudaFree(c->dvar);
     if (c->status) cudaFree(c->status);

@@ -213,3 +213,41 @@ def read_3d_dat(path, nP):
                     except (ValueError, DeckError):
                         raise DeckError(f"Error in reading combined input file at {i + 1} {j + 1} {k + 1}") from None
     return var, time, nstep, x1, x2, x3
+
+
+# ------------------------------------------------- native (library) versions
+def _native():
+    from . import _lib
+    return _lib.load()
+
+
+def write_3d_dat_native(path, var, x1, x2, x3, time=0.0, nstep=0, threads=0):
+    """Same bytes as write_3d_dat, formatted on host threads by the library."""
+    import ctypes
+    from . import _lib
+    L = _native()
+    v = np.ascontiguousarray(var, dtype=np.float64)
+    _, n3, n2, n1 = v.shape
+    nP = (ctypes.c_int32 * 3)(n1, n2, n3)
+    a1, a2, a3 = (np.ascontiguousarray(a, dtype=np.float64) for a in (x1, x2, x3))
+    r = L.chan_deck_write(str(path).encode(), nP, _lib.dptr(v), _lib.dptr(a1), _lib.dptr(a2), _lib.dptr(a3),
+                          float(time), int(nstep), int(threads))
+    if r != 0:
+        raise DeckError(L.chan_io_last_error().decode())
+
+
+def read_3d_dat_native(path, nP, threads=0):
+    """Same result as read_3d_dat, parsed on host threads by the library."""
+    import ctypes
+    from . import _lib
+    L = _native()
+    n1, n2, n3 = nP
+    var = np.empty((7, n3, n2, n1))
+    x1 = np.empty(n1); x2 = np.empty(n2); x3 = np.empty(n3)
+    t = ctypes.c_double(); n = ctypes.c_int64()
+    nPc = (ctypes.c_int32 * 3)(n1, n2, n3)
+    r = L.chan_deck_read(str(path).encode(), nPc, _lib.dptr(var), _lib.dptr(x1), _lib.dptr(x2), _lib.dptr(x3),
+                         ctypes.byref(t), ctypes.byref(n), int(threads))
+    if r != 0:
+        raise DeckError(L.chan_io_last_error().decode())
+    return var, t.value, n.value, x1, x2, x3

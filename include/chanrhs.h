@@ -40,6 +40,7 @@ extern "C" {
 #define CHAN_ENOMEM (-2)   /* device allocation failed */
 #define CHAN_ECUDA (-3)    /* CUDA runtime error (see chan_last_error) */
 #define CHAN_ESTATE (-4)   /* call out of order (e.g. step before upload) */
+#define CHAN_EIO (-5)      /* file error (see chan_last_error / chan_io_last_error) */
 
 #define CHAN_RK2 2         /* the reference's midpoint RK2: maxiter=2, v1.9/codes/comdata.f90:8 */
 #define CHAN_RK3 3         /* SSP-RK3 (Shu-Osher); no reference counterpart */
@@ -158,6 +159,45 @@ const char *chan_last_error(chan_ctx *c);
 
 /* Library version string. */
 const char *chan_version(void);
+
+/* Time averaging of the plane statistics, done on the device.  The reference
+ * appends every statistics step to moment1st/2nd/Joint.dat and tauWall.dat
+ * and time-averages those files offline (v1.9/codes/avg_v1.7.f90:113-274,
+ * avgTauWall.f90).  Here every statistics step (mod(nstep,istat)==0 inside
+ * chan_step) adds its stat1Spc, stat2Spc, corrSpc and tauL, tauU into device
+ * sums once chan_time_avg_start has been called.
+ * chan_time_avg_start: zero the sums and start accumulating.
+ * chan_time_avg: copy out the sums (layouts as chan_stats), the number of
+ * samples and the times of the first and last sample; any pointer may be
+ * NULL.  mean = sum/n; rms = sqrt(sum2/n - mean^2); covariances follow
+ * avg_v1.7.f90:264-274. */
+int chan_time_avg_start(chan_ctx *c);
+int chan_time_avg(chan_ctx *c, double *sum1, double *sum2, double *sumc, double *sumtau, int64_t *nsamples,
+                  double *t0, double *t1);
+
+/* Exact binary checkpoint of a context's device state between time steps:
+ * the conservative state with its periodic ghosts, both wall planes, the
+ * corner columns, the forcing/statistics state and the step counter, time and
+ * time-averaging sums.  Restarting from it continues bit for bit.  The
+ * reference restarts from its Tecplot deck with the forcing reset to zero
+ * (v1.9/codes/main_v1.9.f90:211-282, 749-794); this sidecar has no
+ * counterpart there.  chan_checkpoint_read needs a context of the same grid. */
+int chan_checkpoint_write(chan_ctx *c, const char *path);
+int chan_checkpoint_read(chan_ctx *c, const char *path);
+
+/* The reference's Tecplot-ASCII deck (3D.dat), read and written on host
+ * threads (nthreads <= 0: all hardware threads).  Writer:
+ * v1.9/codes/main_v1.9.f90:759-773 (records 3(1X,F10.6),7(1X,E22.15)).
+ * Reader: main_v1.9.f90:222-251.  var = var(1:nP1,1:nP2,1:nP3,1:7), and
+ * x1(nP1), x2(nP2), x3(nP3) are the coordinate columns (any may be NULL on
+ * read).  A short or malformed record returns CHAN_EIO.  chan_io_last_error
+ * then names the record as the reference does:
+ * "Error in reading combined input file at i j k". */
+int chan_deck_read(const char *path, const int32_t *nP, double *var, double *x1, double *x2, double *x3,
+                   double *time, int64_t *nstep, int32_t nthreads);
+int chan_deck_write(const char *path, const int32_t *nP, const double *var, const double *x1, const double *x2,
+                    const double *x3, double time, int64_t nstep, int32_t nthreads);
+const char *chan_io_last_error(void);
 
 /* Plane moments stat1Spc, stat2Spc, corrSpc of a host field, computed on GPU
  * `device` without allocating any memory.  This entry point has no

@@ -177,3 +177,55 @@ def test_errors_are_codes():
     assert ei.value.code == -4
     with pytest.raises(ChanError):
         Channel(p.with_(nP=(4, 8, 9)), x3[:9], jac[:9], inv[:9])
+
+
+def test_time_averaged_statistics_match_oracle():
+    """Device-side time averaging (avg_v1.7.f90:239-274) against averages of the
+    oracle's plane statistics captured at every statistics step."""
+    from compchan3dmpi_b200.stats import average_snapshots, wall_units
+    p, x3, jac, inv, var = make_case(nP=(24, 16, 21), quantize=False, istat=2)
+    g, o = _pair((p, x3, jac, inv, var))
+    g.time_avg_start()
+    snaps = []
+    for s in range(1, 9):
+        g.step(1)
+        o.step(1)
+        if s % p.istat == 0:
+            snaps.append(tuple(np.array(a) for a in (o.stats()[1], o.stats()[2], o.stats()[3], o.stats()[0])))
+    ta = g.time_average()
+    assert ta["samples"] == len(snaps) == 4
+    mean, rms, covar, tau = average_snapshots(snaps)
+    for a, b in ((ta["mean"], mean), (ta["covar"], covar)):
+        for r in range(a.shape[0]):
+            assert np.max(np.abs(a[r] - b[r])) <= 1e-12 * max(np.max(np.abs(b[r])), 1e-300)
+    np.testing.assert_allclose(ta["rms"], rms, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(ta["tau"], tau, rtol=1e-12, atol=1e-20)
+    w = wall_units(ta["mean"], ta["tau"], x3, p.Re)
+    assert w["Cf"] > 0 and w["u_tau"] > 0
+
+
+def test_checkpoint_restart_is_bit_exact(tmp_path):
+    """8 steps straight == 4 steps, checkpoint, new context, restore, 4 steps."""
+    p, x3, jac, inv, var = make_case(nP=(20, 14, 19), quantize=False, istat=3)
+    a = Channel(p, x3, jac, inv)
+    a.init_sol_v(var)
+    a.time_avg_start()
+    a.step(8)
+    ref = a.download()
+    ref_stats = a.stats()
+    ref_avg = a.time_average()
+    b = Channel(p, x3, jac, inv)
+    b.init_sol_v(var)
+    b.time_avg_start()
+    b.step(4)
+    b.checkpoint_write(tmp_path / "ck.bin")
+    c = Channel(p, x3, jac, inv)
+    c.checkpoint_read(tmp_path / "ck.bin")
+    assert c.nstep == 4
+    c.step(4)
+    assert np.array_equal(c.download(), ref)
+    for x, y in zip(c.stats(), ref_stats):
+        assert np.array_equal(x, y)
+    assert c.time_average()["samples"] == ref_avg["samples"]
+    assert np.array_equal(c.time_average()["mean"], ref_avg["mean"])
+    assert c.nstep == 8 and c.time == a.time

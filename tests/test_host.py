@@ -109,3 +109,78 @@ def test_wall_coeffs_sum_to_zero():
     c = wall_coeffs(x3)
     assert abs(c["f1d2c0"] + c["f1d2c1"] + c["f1d2c2"]) < 1e-9 * abs(c["f1d2c0"])
     assert abs(c["b1d2c0"] + c["b1d2c1"] + c["b1d2c2"]) < 1e-9 * abs(c["b1d2c0"])
+
+
+def test_wall_units_laminar_known_answer():
+    """Poiseuille u = 1.5(1-(z-1)^2), rho = T = 1: tau_w = mu*du/dz/Re = 3/Re,
+    U_b = 1, so Cf = 6/Re and u_tau = sqrt(3/Re)."""
+    from compchan3dmpi_b200.stats import wall_units
+    x3, _, _ = mesh_cosine(401)
+    Re = 3000.0
+    mean = np.zeros((7, x3.size))
+    mean[0] = 1.0
+    mean[1] = 1.5 * (1 - (x3 - 1) ** 2)
+    w = wall_units(mean, np.array([3.0 / Re, -3.0 / Re]), x3, Re)
+    assert abs(w["Cf"] - 6.0 / Re) < 1e-4 * (6.0 / Re)   # trapezoidal U_b on 401 points
+    assert abs(w["u_tau"] - math.sqrt(3.0 / Re)) < 1e-15
+    assert abs(w["Re_tau"] - math.sqrt(3.0 * Re)) < 1e-9
+    assert w["yplus"][0] == 0.0 and w["uplus"][0] == 0.0
+
+
+def test_time_average_formulas_and_series_roundtrip(tmp_path):
+    """avg_v1.7.f90:239-274 on synthetic snapshots; series files in the reference's F15.7 format."""
+    from compchan3dmpi_b200.stats import average_snapshots, append_series, read_series, write_profiles
+    rng = np.random.default_rng(3)
+    n3 = 6
+    snaps = []
+    for s in range(4):
+        s1 = rng.uniform(0.5, 1.5, (7, n3)); s2 = s1 ** 2 + rng.uniform(0, 0.1, (7, n3))
+        c = rng.uniform(0, 1, (9, n3)); tau = rng.uniform(-1e-3, 1e-3, 2)
+        snaps.append((s1, s2, c, tau))
+        append_series(tmp_path, 0.1 * (s + 1), tau, s1, s2, c)
+    mean, rms, covar, tau = average_snapshots(snaps)
+    m1 = sum(s[0] for s in snaps) / 4
+    assert np.allclose(mean, m1)
+    assert np.allclose(rms, np.sqrt(sum(s[1] for s in snaps) / 4 - m1 ** 2))
+    assert np.allclose(covar[2], sum(s[2][2] for s in snaps) / 4 - m1[1] * m1[2])
+    t, v = read_series(tmp_path / "moment1st.dat", 7, n3)
+    assert np.allclose(t, [0.1, 0.2, 0.3, 0.4]) and np.allclose(v[0], snaps[0][0], atol=5e-8)
+    write_profiles(tmp_path, np.linspace(0, 2, n3), mean, rms, covar)
+    assert len((tmp_path / "mean.dat").read_text().splitlines()) == n3
+
+
+def test_native_deck_matches_python_byte_for_byte(tmp_path):
+    from compchan3dmpi_b200.deck import write_3d_dat_native, read_3d_dat_native
+    p = ChanParams(nP=(9, 6, 7))
+    x3, _, _ = mesh_cosine(7)
+    v = quantize_deck(laminar_noise(p, x3))
+    v[4, 3, 2, 1] = -1.2345678901234567e-120   # three-digit exponent form
+    v[2, 0, 0, 0] = 0.0
+    x1, x2 = periodic_coords(9, p.Lx), periodic_coords(6, p.Ly)
+    write_3d_dat(tmp_path / "py.dat", v, x1, x2, x3, 0.375, 17)
+    write_3d_dat_native(tmp_path / "c.dat", v, x1, x2, x3, 0.375, 17, threads=3)
+    assert (tmp_path / "py.dat").read_bytes() == (tmp_path / "c.dat").read_bytes()
+    back, t, n, bx1, bx2, bx3 = read_3d_dat_native(tmp_path / "c.dat", p.nP, threads=2)
+    pyb, pt, pn, *_ = read_3d_dat(tmp_path / "c.dat", p.nP)
+    assert np.array_equal(back, pyb) and t == pt == 0.375 and n == pn == 17
+    assert np.allclose(bx3, x3, atol=1e-6) and np.allclose(bx1, x1, atol=1e-6)
+
+
+def test_native_deck_reports_bad_records(tmp_path):
+    from compchan3dmpi_b200.deck import write_3d_dat_native, read_3d_dat_native
+    p = ChanParams(nP=(6, 6, 7))
+    x3, _, _ = mesh_cosine(7)
+    v = laminar_noise(p, x3)
+    f = tmp_path / "3D.dat"
+    write_3d_dat_native(f, v, periodic_coords(6, p.Lx), periodic_coords(6, p.Ly), x3)
+    lines = f.read_text().splitlines()
+    (tmp_path / "short.dat").write_text("\n".join(lines[:50]) + "\n")
+    with pytest.raises(DeckError, match="Error in reading combined input file at"):
+        read_3d_dat_native(tmp_path / "short.dat", p.nP)
+    bad = lines[:]
+    bad[12] = bad[12][:60] + "#" + bad[12][61:]
+    (tmp_path / "bad.dat").write_text("\n".join(bad) + "\n")
+    with pytest.raises(DeckError, match="Error in reading combined input file at 1 2 1"):   # line 12 = i1 j2 k1
+        read_3d_dat_native(tmp_path / "bad.dat", p.nP)
+    with pytest.raises(DeckError, match="cannot open"):
+        read_3d_dat_native(tmp_path / "missing.dat", p.nP)
