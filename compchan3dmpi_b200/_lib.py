@@ -22,6 +22,21 @@ _I32 = ctypes.POINTER(ctypes.c_int32)
 _I64 = ctypes.POINTER(ctypes.c_int64)
 
 
+class ChanWallBCC(ctypes.Structure):
+    """Mirror of ``struct chan_wall_bc``."""
+    _fields_ = [
+        ("velocity", ctypes.c_int32),
+        ("thermal", ctypes.c_int32),
+        ("Tw", ctypes.c_double),
+        ("dTdz", ctypes.c_double),
+        ("slip_grad", ctypes.c_double),
+        ("wave", ctypes.c_double * 4),
+        ("mask", ctypes.POINTER(ctypes.c_uint8)),
+        ("uv", ctypes.POINTER(ctypes.c_double)),
+        ("x1", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 class ChanParamsC(ctypes.Structure):
     """Mirror of ``struct chan_params``."""
     _fields_ = [
@@ -67,6 +82,7 @@ SIGNATURES = [
     ("chan_version", ctypes.c_char_p, []),
     ("chan_time_avg_start", ctypes.c_int, [ctypes.c_void_p]),
     ("chan_time_avg", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _I64, _D, _D]),
+    ("chan_set_wall_bc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ChanWallBCC)]),
     ("chan_checkpoint_write", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_checkpoint_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_deck_read", ctypes.c_int, [ctypes.c_char_p, _I32, _D, _D, _D, _D, _D, _I64, ctypes.c_int32]),

@@ -170,6 +170,24 @@ class Channel:
         return {"mean": mean, "rms": rms, "covar": covar, "tau": tau, "samples": n.value,
                 "t0": t0.value, "t1": t1.value}
 
+    def set_wall_bc(self, wall: int, bc):
+        """Wall-BC plug-in for wall 0 (k=1) or 1 (k=nP3); ``bc`` is a wallbc.WallBC."""
+        c = _lib.ChanWallBCC()
+        c.velocity = int(bc.velocity); c.thermal = int(bc.thermal)
+        c.Tw = float(bc.Tw); c.dTdz = float(bc.dTdz); c.slip_grad = float(bc.slip_grad)
+        c.wave[:] = [float(x) for x in bc.wave]
+        keep = []
+        if bc.mask is not None:
+            m = np.ascontiguousarray(bc.mask, dtype=np.uint8); keep.append(m)
+            c.mask = m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        if bc.uv is not None:
+            uv = np.ascontiguousarray(bc.uv, dtype=np.float64); keep.append(uv)
+            c.uv = _lib.dptr(uv)
+        if bc.x1 is not None:
+            x1 = np.ascontiguousarray(bc.x1, dtype=np.float64); keep.append(x1)
+            c.x1 = _lib.dptr(x1)
+        self._check(self.L.chan_set_wall_bc(self._h, int(wall), ctypes.byref(c)))
+
     def set_forcing(self, tauL: float, tauU: float, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         self._check(self.L.chan_set_forcing(self._h, float(tauL), float(tauU), _lib.dptr(rb)))

@@ -32,6 +32,19 @@ struct DevStatus {
     long long pad;
 };
 
+// Boundary condition of one wall plane (plug-in of the reference's wall-BC
+// variants in v1.9_strat, v1.9_groov, v1.9_groov_strat, v1.9_STWNV and v1.9_RD, lines ~605-640).
+struct WallBC {
+    int vel;              // 0 no-slip; 1 slip mask: c0*u1+c1*u2+c2*u3 = g where mask, else no-slip;
+                          // 2 prescribed (u_w, v_w) field; 3 wave v_w = A sin(k x1 + om t + ph*(j odd))
+    int therm;            // 0 isothermal Tw; 1 fixed one-sided gradient c0*T1+c1*T2+c2*T3 = dTdz
+    double Tw, dTdz, g;
+    double A, kx, om, ph;
+    const unsigned char *mask;  // [nP2][nP1], 1-based (i,j) at (j-1)*nP1 + i-1
+    const double *uv;           // [2][nP2][nP1]
+    const double *x1;           // [nP1] x coordinates for the wave
+};
+
 struct KParams {
     // geometry
     int n1, n2, n3, px, NJ, kchunk;
@@ -64,6 +77,9 @@ struct KParams {
     int check;            // last stage of a step: run the blow-up test
     int force_on;
     int acc_on;           // statistics steps also add into tacc (time averaging)
+    int wall_custom;      // any wall uses a non-default WallBC
+    WallBC wbc[2];
+    double time;          // time of the step being computed (the reference's `time`)
     long long step;       // step number being computed
 };
 
@@ -666,6 +682,57 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 // ---------------------------------------------------------------------------
 // Wall BC + pressure BC (main_v1.9.f90:623-720 on the two wall planes).
 // One thread per (i,j) of a wall plane, ghosts included.
+
+// var(u, v, T) of an interior point as the reference holds it (corner columns
+// keep their stale values)
+__device__ __forceinline__ void inner_uvT(const KParams &P, int i, int j, int k, double &u, double &v, double &T)
+{
+    const int n1 = P.n1, n2 = P.n2;
+    if ((i == 1 || i == n1) && (j == 1 || j == n2)) {
+        const double *C = P.cs + ((size_t)k * 4 + (i == 1 ? 0 : 1) + (j == 1 ? 0 : 2)) * 7;
+        u = C[1]; v = C[2]; T = C[5];
+        return;
+    }
+    const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+    const double q0 = P.qout[o];
+    u = P.qout[P.vol + o] / q0;
+    v = P.qout[2 * P.vol + o] / q0;
+    const double w = P.qout[3 * P.vol + o] / q0;
+    const double E = P.qout[4 * P.vol + o] / q0;
+    T = E - P.ggMh * ((u * u + v * v) + w * w);
+}
+
+// wall values u, v, T of point (i,j) of wall `wall` after the wall BC
+__device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, double &v, double &T)
+{
+    const WallBC &B = P.wbc[wall];
+    const int n1 = P.n1, n2 = P.n2;
+    const int ic = i < 1 ? 1 : (i > n1 ? n1 : i), jc = j < 1 ? 1 : (j > n2 ? n2 : j);
+    const int k2 = wall == 0 ? 2 : P.n3 - 1, k3 = wall == 0 ? 3 : P.n3 - 2;
+    const double *c = wall == 0 ? P.f1 : P.b1;
+    u = 0.0;
+    v = 0.0;
+    double u2 = 0, v2 = 0, T2 = 0, u3 = 0, v3 = 0, T3 = 0;
+    const bool need_inner = (B.vel == 1 && B.mask[(jc - 1) * n1 + ic - 1]) || B.therm == 1;
+    if (need_inner) {
+        inner_uvT(P, ic, jc, k2, u2, v2, T2);
+        inner_uvT(P, ic, jc, k3, u3, v3, T3);
+    }
+    if (B.vel == 1) {
+        if (B.mask[(jc - 1) * n1 + ic - 1]) {
+            u = ((B.g - c[1] * u2) - c[2] * u3) / c[0];
+            v = ((B.g - c[1] * v2) - c[2] * v3) / c[0];
+        }
+    } else if (B.vel == 2) {
+        u = B.uv[(jc - 1) * n1 + ic - 1];
+        v = B.uv[n1 * n2 + (jc - 1) * n1 + ic - 1];
+    } else if (B.vel == 3) {
+        const double x = B.x1[ic - 1];
+        v = B.A * sin((B.kx * x + B.om * P.time) + ((jc & 1) ? B.ph : 0.0));
+    }
+    T = (B.therm == 1) ? ((B.dTdz - c[1] * T2) - c[2] * T3) / c[0] : B.Tw;
+}
+
 __global__ void k_wall(const KParams P)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,7 +744,13 @@ __global__ void k_wall(const KParams P)
     const long long plane = P.plane, vol = P.vol;
     double *W = P.wp + (size_t)wall * 8 * plane;
     const long long idx = (long long)j * P.px + i;
-    const double Tw = wall == 0 ? P.Twb : P.Twt;
+    const bool custom = P.wall_custom != 0;
+    double uw = 0.0, vw = 0.0, Tw = wall == 0 ? P.Twb : P.Twt;
+    double muw = wall == 0 ? P.muwb : P.muwt;
+    if (custom) {
+        wall_point(P, wall, i, j, uw, vw, Tw);
+        if (P.wbc[wall].therm == 1) muw = pow07(Tw);
+    }
     const double pold = W[6 * plane + idx];
     const double rho = (P.gM2 * pold) / Tw;   // gama*Mac**2*p/T with the previous p
     double pnew = pold;
@@ -699,6 +772,19 @@ __global__ void k_wall(const KParams P)
             p = (r * T) / P.gM2;
             mu = pow(T, 0.7);
         };
+        // wall-point terms c0*mu_w*u_w of the neighbours (zero for a no-slip wall)
+        double t_ip = 0.0, t_im = 0.0, t_jp = 0.0, t_jm = 0.0;
+        if (custom) {
+            double u, v, T;
+            wall_point(P, wall, i + 1, j, u, v, T);
+            t_ip = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * u;
+            wall_point(P, wall, i - 1, j, u, v, T);
+            t_im = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * u;
+            wall_point(P, wall, i, j + 1, u, v, T);
+            t_jp = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * v;
+            wall_point(P, wall, i, j - 1, u, v, T);
+            t_jm = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * v;
+        }
         double r, u, v, w, T, p, mu;
         double a2, a3, b2, b3;
         // d/dx of mu*du/dz
@@ -706,31 +792,31 @@ __global__ void k_wall(const KParams P)
         prim(i + 1, j, k3, r, u, v, w, T, p, mu); a3 = c1[2] * mu * u;
         prim(i - 1, j, k2, r, u, v, w, T, p, mu); b2 = c1[1] * mu * u;
         prim(i - 1, j, k3, r, u, v, w, T, p, mu); b3 = c1[2] * mu * u;
-        const double dudxdz = ((a2 + a3) - (b2 + b3)) * P.hdx;
+        const double dudxdz = (((t_ip + a2) + a3) - ((t_im + b2) + b3)) * P.hdx;
         prim(i, j + 1, k2, r, u, v, w, T, p, mu); a2 = c1[1] * mu * v;
         prim(i, j + 1, k3, r, u, v, w, T, p, mu); a3 = c1[2] * mu * v;
         prim(i, j - 1, k2, r, u, v, w, T, p, mu); b2 = c1[1] * mu * v;
         prim(i, j - 1, k3, r, u, v, w, T, p, mu); b3 = c1[2] * mu * v;
-        const double dvdydz = ((a2 + a3) - (b2 + b3)) * P.hdy;
+        const double dvdydz = (((t_jp + a2) + a3) - ((t_jm + b2) + b3)) * P.hdy;
         double p2, p3, d2, d3, e2, e3;
         prim(i, j, k2, r, u, v, w, T, p, mu);
         d2 = c2[1] * mu * w; e2 = c1[1] * r * (w * w); p2 = p;
         prim(i, j, k3, r, u, v, w, T, p, mu);
         d3 = c2[2] * mu * w; e3 = c1[2] * r * (w * w); p3 = p;
-        // the wall-point terms vanish: u=v=w=0 there after the wall BC
+        // the wall-point w terms vanish: w = 0 on every wall
         const double d2wdz2 = d2 + d3;
         const double drhow2dz = e2 + e3;
         const double lhs = P.invRe * ((-dudxdz - dvdydz) + P.two3rd * ((dudxdz + dvdydz) - 2.0 * d2wdz2)) + drhow2dz;
         pnew = -((lhs + c1[1] * p2) + c1[2] * p3) / c1[0];
     }
     W[0 * plane + idx] = rho;
-    W[1 * plane + idx] = 0.0;
-    W[2 * plane + idx] = 0.0;
+    W[1 * plane + idx] = uw;
+    W[2 * plane + idx] = vw;
     W[3 * plane + idx] = 0.0;
-    W[4 * plane + idx] = Tw;
+    W[4 * plane + idx] = custom ? Tw + P.ggMh * ((uw * uw + vw * vw) + 0.0) : Tw;
     W[5 * plane + idx] = Tw;
     W[6 * plane + idx] = pnew;
-    W[7 * plane + idx] = wall == 0 ? P.muwb : P.muwt;
+    W[7 * plane + idx] = muw;
     if (P.check && i >= 1 && i <= n1 && j >= 1 && j <= n2) {
         if (rho < 0.0 || Tw < 0.0) flag_blown(P.status, i, j, wall == 0 ? 1 : n3, P.step);
         if (!isfinite(rho) || !isfinite(pnew)) flag_nonfinite(P.status, i, j, wall == 0 ? 1 : n3);

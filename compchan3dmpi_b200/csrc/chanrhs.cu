@@ -41,6 +41,8 @@ struct chan_ctx {
     chan::KParams kp{};
     double *q[3] = {nullptr, nullptr, nullptr};
     double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr, *tacc = nullptr;
+    unsigned char *wmask[2] = {nullptr, nullptr};  // wall-BC plug-in arrays (allocated on first use)
+    double *wuv[2] = {nullptr, nullptr}, *wx1[2] = {nullptr, nullptr};
     long long tavg_samples = 0;  // statistics steps summed into tacc since chan_time_avg_start
     double tavg_t0 = 0.0, tavg_t1 = 0.0;
     chan::DevStatus *status = nullptr;
@@ -168,9 +170,10 @@ void set_stage(chan_ctx *c, int iter)
     }
 }
 
-int launch_stage(chan_ctx *c, int iter, bool check, long long step)
+int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
 {
     set_stage(c, iter);
+    c->kp.time = time;
     c->cur = c->kp.qout == c->q[0] ? 0 : (c->kp.qout == c->q[1] ? 1 : 2);
     c->kp.check = check ? 1 : 0;
     c->kp.step = step;
@@ -204,7 +207,7 @@ int enqueue_steps(chan_ctx *c, int nsteps)
     for (int s = 0; s < nsteps; s++) {
         const long long step = c->nstep + 1;
         for (int it = 1; it <= c->nstage; it++) {
-            int r = launch_stage(c, it, it == c->nstage, step);
+            int r = launch_stage(c, it, it == c->nstage, step, c->time + c->p.dt);
             if (r) return r;
         }
         c->nstep = step;
@@ -447,6 +450,11 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
         k.f1[m] = co[m]; k.f2[m] = co[3 + m]; k.b1[m] = co[6 + m]; k.b2[m] = co[9 + m];
     }
     k.force_on = p->forcing == CHAN_FORCE_WALLSHEAR ? 1 : 0;
+    k.wall_custom = 0;
+    for (int w = 0; w < 2; w++) {
+        k.wbc[w] = chan::WallBC{};
+        k.wbc[w].Tw = p->Tw[w];
+    }
 
     // stage-kernel launch shape: tiles x k-chunks filling whole waves
     c->ntx = (n1 - 2 + TI - 1) / TI;
@@ -516,7 +524,7 @@ int chan_stage(chan_ctx *c, int iter)
     if (!c->uploaded) { c->err = "chan_stage before chan_upload"; return CHAN_ESTATE; }
     if (iter < 1 || iter > c->nstage) { c->err = "iter out of range"; return CHAN_EINVAL; }
     CK(c, cudaSetDevice(c->dev));
-    int r = launch_stage(c, iter, iter == c->nstage, c->nstep + 1);
+    int r = launch_stage(c, iter, iter == c->nstage, c->nstep + 1, c->time + c->p.dt);
     if (r) return r;
     return read_status(c, nullptr);
 }
@@ -766,6 +774,56 @@ int chan_checkpoint_read(chan_ctx *c, const char *path)
     return CHAN_OK;
 }
 
+int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc)
+{
+    if (!c || !bc || wall < 0 || wall > 1) return CHAN_EINVAL;
+    if (bc->velocity < CHAN_WALL_NOSLIP || bc->velocity > CHAN_WALL_WAVE ||
+        (bc->thermal != CHAN_WALL_ISOTHERMAL && bc->thermal != CHAN_WALL_FIXED_GRADIENT)) {
+        c->err = "bad wall-BC kind";
+        return CHAN_EINVAL;
+    }
+    if ((bc->velocity == CHAN_WALL_SLIP_MASK && !bc->mask) || (bc->velocity == CHAN_WALL_UV_FIELD && !bc->uv)) {
+        c->err = "wall-BC kind needs its mask / uv array";
+        return CHAN_EINVAL;
+    }
+    if (bc->thermal == CHAN_WALL_ISOTHERMAL && !(bc->Tw > 0)) { c->err = "Tw must be > 0"; return CHAN_EINVAL; }
+    CK(c, cudaSetDevice(c->dev));
+    const size_t n12 = (size_t)c->n1 * c->n2;
+    if (!c->wmask[wall]) {
+        CK(c, cudaMalloc((void **)&c->wmask[wall], n12));
+        CK(c, cudaMalloc((void **)&c->wuv[wall], 2 * n12 * sizeof(double)));
+        CK(c, cudaMalloc((void **)&c->wx1[wall], (size_t)c->n1 * sizeof(double)));
+        c->dev_bytes += n12 + 2 * n12 * sizeof(double) + (size_t)c->n1 * sizeof(double);
+    }
+    if (bc->mask) CK(c, cudaMemcpy(c->wmask[wall], bc->mask, n12, cudaMemcpyHostToDevice));
+    if (bc->uv) CK(c, cudaMemcpy(c->wuv[wall], bc->uv, 2 * n12 * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> x1(c->n1);
+    if (bc->x1) {
+        for (int i = 0; i < c->n1; i++) x1[i] = bc->x1[i];
+    } else {  // x1(1)=0, x1(i+1)=x1(i)+dx (v1.9/codes/comdata.f90:93-95)
+        const double dx = c->p.Lx / (double)(c->n1 - 1);
+        x1[0] = 0.0;
+        for (int i = 1; i < c->n1; i++) x1[i] = x1[i - 1] + dx;
+    }
+    CK(c, cudaMemcpy(c->wx1[wall], x1.data(), x1.size() * sizeof(double), cudaMemcpyHostToDevice));
+    chan::WallBC &W = c->kp.wbc[wall];
+    W.vel = bc->velocity;
+    W.therm = bc->thermal;
+    W.Tw = bc->Tw;
+    W.dTdz = bc->dTdz;
+    W.g = bc->slip_grad;
+    W.A = bc->wave[0]; W.kx = bc->wave[1]; W.om = bc->wave[2]; W.ph = bc->wave[3];
+    W.mask = c->wmask[wall];
+    W.uv = c->wuv[wall];
+    W.x1 = c->wx1[wall];
+    if (wall == 0) { c->kp.Twb = bc->Tw; c->kp.muwb = pow(bc->Tw, 0.7); }
+    else { c->kp.Twt = bc->Tw; c->kp.muwt = pow(bc->Tw, 0.7); }
+    c->kp.wall_custom = 0;
+    for (int w = 0; w < 2; w++)
+        if (c->kp.wbc[w].vel != 0 || c->kp.wbc[w].therm != 0) c->kp.wall_custom = 1;
+    return CHAN_OK;
+}
+
 int chan_time_avg_start(chan_ctx *c)
 {
     if (!c) return CHAN_EINVAL;
@@ -856,6 +914,11 @@ void chan_free(chan_ctx *c)
     if (c->cs) cudaFree(c->cs);
     if (c->tabs) cudaFree(c->tabs);
     if (c->tacc) cudaFree(c->tacc);
+    for (int w = 0; w < 2; w++) {
+        if (c->wmask[w]) cudaFree(c->wmask[w]);
+        if (c->wuv[w]) cudaFree(c->wuv[w]);
+        if (c->wx1[w]) cudaFree(c->wx1[w]);
+    }
     if (c->stat) cudaFree(c->stat);
     if (c->dvar) cudaFree(c->dvar);
     if (c->status) cudaFree(c->status);

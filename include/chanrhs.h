@@ -175,6 +175,40 @@ int chan_time_avg_start(chan_ctx *c);
 int chan_time_avg(chan_ctx *c, double *sum1, double *sum2, double *sumc, double *sumtau, int64_t *nsamples,
                   double *t0, double *t1);
 
+/* Wall boundary-condition plug-in.  It covers the reference's wall-BC
+ * variants, which differ only in the wall block of the stage
+ * (v1.9/codes/main_v1.9.f90:623-641):
+ *   isothermal T_w        v1.9_strat/v1.9_st1,st2 (T_w = 0.2, 1.8)
+ *   fixed dT/dz           v1.9_strat/v1.9_st3,st4: c0*T1 + c1*T2 + c2*T3 = dTdz
+ *   slip mask             v1.9_groov, v1.9_groov_strat variants: where mask != 0,
+ *                         c0*u1 + c1*u2 + c2*u3 = slip_grad (same for v), else u = v = 0
+ *   prescribed (u,v)      v1.9_RD variants, rotating discs (field built by the caller)
+ *   travelling wave       v1.9_STWNV variants: v_w = A*sin(k*x1(i) + omega*time + phase*(j odd))
+ * c0..c2 are the one-sided coefficients of that wall (f1d2 bottom, b1d2 top),
+ * w_w = 0 always, and the pressure BC includes the wall velocity terms.
+ * The default of both walls is no-slip and isothermal at chan_params.Tw.
+ * mask, uv and x1 are copied; x1 (nP1 values) may be NULL to use
+ * x1(i) = (i-1)*Lx/(nP1-1) accumulated as comdata.f90:93-95.  A travelling
+ * wave uses the time of the step being computed. */
+#define CHAN_WALL_NOSLIP 0
+#define CHAN_WALL_SLIP_MASK 1
+#define CHAN_WALL_UV_FIELD 2
+#define CHAN_WALL_WAVE 3
+#define CHAN_WALL_ISOTHERMAL 0
+#define CHAN_WALL_FIXED_GRADIENT 1
+typedef struct chan_wall_bc {
+    int32_t velocity;         /* CHAN_WALL_NOSLIP .. CHAN_WALL_WAVE */
+    int32_t thermal;          /* CHAN_WALL_ISOTHERMAL or CHAN_WALL_FIXED_GRADIENT */
+    double Tw;                /* isothermal wall temperature */
+    double dTdz;              /* fixed one-sided wall-normal temperature gradient */
+    double slip_grad;         /* one-sided du/dz = dv/dz on slip points */
+    double wave[4];           /* A, k, omega, phase added on odd j (1-based) */
+    const uint8_t *mask;      /* nP1*nP2, i fastest: nonzero = slip */
+    const double *uv;         /* u_w then v_w, each nP1*nP2, i fastest */
+    const double *x1;         /* nP1 streamwise coordinates for the wave, or NULL */
+} chan_wall_bc;
+int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc);
+
 /* Exact binary checkpoint of a context's device state between time steps:
  * the conservative state with its periodic ghosts, both wall planes, the
  * corner columns, the forcing/statistics state and the step counter, time and

@@ -73,7 +73,13 @@ typedef struct {
     double *stat1, *stat2, *corr;/* [7][n3], [7][n3], [9][n3] (k fastest, 0-based k) */
     long nstep;
     double time;
+    double tstage;       /* time seen by the wall BC during a stage (the step's new time) */
     int blown, blown_ijk[3];
+    /* wall-BC variants (see orc_set_wall_bc) */
+    int wvel[2], wtherm[2];
+    double wTw[2], wdTdz[2], wg[2], wwave[2][4];
+    unsigned char *wmask[2];
+    double *wuv[2], *wx1[2];
 } orc_t;
 
 #define ID(o, i, j, k) ((((size_t)(k)) * (o)->NJ + (size_t)(j)) * (o)->NI + (size_t)(i))
@@ -155,6 +161,7 @@ void orc_free(orc_t *o)
     free(o->fD); free(o->gD); free(o->hD);
     free(o->F1); free(o->G1); free(o->H1);
     free(o->stat1); free(o->stat2); free(o->corr);
+    for (int w = 0; w < 2; w++) { free(o->wmask[w]); free(o->wuv[w]); free(o->wx1[w]); }
     free(o);
 }
 
@@ -176,6 +183,7 @@ orc_t *orc_create(const int *nP, const double *prm, const double *x3,
     o->invPr = 1.0 / prm[P_PR];           /* comdata.f90:12 invPr=1/0.71 */
     o->PexVal = prm[P_PEX]; o->PeyVal = prm[P_PEY]; o->PezVal = prm[P_PEZ];
     o->Twb = prm[P_TWB]; o->Twt = prm[P_TWT];
+    o->wTw[0] = o->Twb; o->wTw[1] = o->Twt;
     o->istat = (int)prm[P_ISTAT]; o->rk = (int)prm[P_RK]; o->forcing = (int)prm[P_FORCING];
     o->invRe = 1.0 / o->Re;               /* comdata.f90:59 */
     o->ggM = o->gama * (o->gama - 1) * (o->Mac * o->Mac); /* comdata.f90:60 */
@@ -292,6 +300,7 @@ void orc_upload(orc_t *o, const double *v, long nstep, double time)
     share2P(o, o->var, 7);
     o->nstep = nstep;
     o->time = time;
+    o->tstage = time + o->dt;
     o->tauL = 0.0; o->tauU = 0.0;       /* never set before the first stats step */
     memset(o->stat1, 0, sizeof(double) * 7 * n3);
     o->blown = 0;
@@ -530,18 +539,36 @@ void orc_stage(orc_t *o, int iter)
     }
     share2P(o, o->var, 7);
 
-    /* ---- wall boundary conditions: main19fix:623-641 */
+    /* ---- wall boundary conditions: main19fix:623-641, with the wall-BC
+     * variants of v1.9_strat (st1-st4: T_w, fixed dT/dz), v1.9_groov and
+     * v1.9_groov_strat (slip stripes), v1.9_STWNV (s1-s6: travelling wave v_w)
+     * and v1.9_RD (rd1-rd3: prescribed disc velocity), lines ~605-640 there. */
     {
         int i, j;
         for (j = 1; j <= n2; j++)
             for (i = 1; i <= n1; i++) {
                 int kw;
                 for (kw = 0; kw < 2; kw++) {
-                    int kk = kw == 0 ? 1 : n3;
-                    double Tw = kw == 0 ? o->Twb : o->Twt;
+                    const int kk = kw == 0 ? 1 : n3, k2 = kw == 0 ? 2 : n3 - 1, k3 = kw == 0 ? 3 : n3 - 2;
+                    const double c0 = kw == 0 ? o->f1d2c0 : o->b1d2c0, c1 = kw == 0 ? o->f1d2c1 : o->b1d2c1;
+                    const double c2 = kw == 0 ? o->f1d2c2 : o->b1d2c2;
+                    const size_t pi = (size_t)(j - 1) * n1 + (i - 1);
                     double s;
                     VAR(o, 2, i, j, kk) = 0.0; VAR(o, 3, i, j, kk) = 0.0; VAR(o, 4, i, j, kk) = 0.0;
-                    VAR(o, 6, i, j, kk) = Tw;
+                    if (o->wvel[kw] == 1 && o->wmask[kw][pi]) {
+                        VAR(o, 2, i, j, kk) = (o->wg[kw] - c1 * VAR(o, 2, i, j, k2) - c2 * VAR(o, 2, i, j, k3)) / c0;
+                        VAR(o, 3, i, j, kk) = (o->wg[kw] - c1 * VAR(o, 3, i, j, k2) - c2 * VAR(o, 3, i, j, k3)) / c0;
+                    } else if (o->wvel[kw] == 2) {
+                        VAR(o, 2, i, j, kk) = o->wuv[kw][pi];
+                        VAR(o, 3, i, j, kk) = o->wuv[kw][(size_t)n1 * n2 + pi];
+                    } else if (o->wvel[kw] == 3) {
+                        VAR(o, 3, i, j, kk) = o->wwave[kw][0] *
+                            sin(o->wwave[kw][1] * o->wx1[kw][i - 1] + o->wwave[kw][2] * o->tstage + ((j & 1) ? o->wwave[kw][3] : 0.0));
+                    }
+                    if (o->wtherm[kw] == 1)
+                        VAR(o, 6, i, j, kk) = (o->wdTdz[kw] - c1 * VAR(o, 6, i, j, k2) - c2 * VAR(o, 6, i, j, k3)) / c0;
+                    else
+                        VAR(o, 6, i, j, kk) = o->wTw[kw];
                     s = VAR(o, 2, i, j, kk) * VAR(o, 2, i, j, kk) + VAR(o, 3, i, j, kk) * VAR(o, 3, i, j, kk)
                         + VAR(o, 4, i, j, kk) * VAR(o, 4, i, j, kk);
                     VAR(o, 5, i, j, kk) = VAR(o, 6, i, j, kk) + ggM * haf * s;
@@ -704,7 +731,9 @@ int orc_step(orc_t *o, int nsteps)
     for (s = 0; s < nsteps; s++) {
         o->nstep = o->nstep + 1;
         o->time = o->time + o->dt;
+        o->tstage = o->time;
         for (iter = 1; iter <= nstage; iter++) orc_stage(o, iter);
+        o->tstage = o->time + o->dt;   /* a stage run alone belongs to the next step */
         if (orc_check(o)) return 1;
         if (o->istat > 0 && o->nstep % o->istat == 0) {
             orc_tau_wall(o);
@@ -712,6 +741,28 @@ int orc_step(orc_t *o, int nsteps)
         }
     }
     return 0;
+}
+
+/* Wall-BC variant of wall w (0 bottom, 1 top).  vel: 0 no-slip, 1 slip mask
+ * (c0*u1+c1*u2+c2*u3 = g), 2 prescribed uv field, 3 travelling wave
+ * v = A sin(k x1 + om t + ph*(j odd)); therm: 0 isothermal Tw, 1 fixed dT/dz.
+ * mask/uv are nP1*nP2 (i fastest), uv holds u then v; x1 has nP1 values. */
+void orc_set_wall_bc(orc_t *o, int w, int vel, int therm, double Tw, double dTdz, double g, const double *wave,
+                     const unsigned char *mask, const double *uv, const double *x1)
+{
+    const size_t n12 = (size_t)o->n1 * o->n2;
+    o->wvel[w] = vel; o->wtherm[w] = therm; o->wTw[w] = Tw; o->wdTdz[w] = dTdz; o->wg[w] = g;
+    for (int m = 0; m < 4; m++) o->wwave[w][m] = wave ? wave[m] : 0.0;
+    if (!o->wmask[w]) {
+        o->wmask[w] = (unsigned char *)calloc(n12, 1);
+        o->wuv[w] = (double *)calloc(2 * n12, sizeof(double));
+        o->wx1[w] = (double *)calloc((size_t)o->n1, sizeof(double));
+    }
+    if (mask) memcpy(o->wmask[w], mask, n12);
+    if (uv) memcpy(o->wuv[w], uv, 2 * n12 * sizeof(double));
+    if (x1) memcpy(o->wx1[w], x1, sizeof(double) * (size_t)o->n1);
+    else { o->wx1[w][0] = 0.0; for (int i = 1; i < o->n1; i++) o->wx1[w][i] = o->wx1[w][i - 1] + o->dx; }
+    if (w == 0) o->Twb = Tw; else o->Twt = Tw;
 }
 
 /* ------------------------------------------------------------ accessors */

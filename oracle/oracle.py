@@ -67,6 +67,8 @@ def lib():
         L.orc_download_solv.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
         L.orc_get_stats.argtypes = [ctypes.c_void_p, _D, _D, _D, _D]
         L.orc_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D]
+        L.orc_set_wall_bc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, _D, ctypes.c_void_p, _D, _D]
         L.orc_nstep.argtypes = [ctypes.c_void_p]
         L.orc_nstep.restype = ctypes.c_long
         L.orc_time.argtypes = [ctypes.c_void_p]
@@ -180,6 +182,16 @@ class Oracle:
     def set_forcing(self, tauL, tauU, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         lib().orc_set_forcing(self._h, float(tauL), float(tauU), _dp(rb))
+
+    def set_wall_bc(self, wall, bc):
+        """Same WallBC description as Channel.set_wall_bc."""
+        wave = np.ascontiguousarray(bc.wave, dtype=np.float64)
+        mask = None if bc.mask is None else np.ascontiguousarray(bc.mask, dtype=np.uint8)
+        uv = None if bc.uv is None else np.ascontiguousarray(bc.uv, dtype=np.float64)
+        x1 = None if bc.x1 is None else np.ascontiguousarray(bc.x1, dtype=np.float64)
+        lib().orc_set_wall_bc(self._h, int(wall), int(bc.velocity), int(bc.thermal), float(bc.Tw), float(bc.dTdz),
+                              float(bc.slip_grad), _dp(wave), None if mask is None else mask.ctypes.data,
+                              None if uv is None else _dp(uv), None if x1 is None else _dp(x1))
 
     @property
     def nstep(self):
