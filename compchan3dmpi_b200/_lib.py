@@ -83,6 +83,13 @@ SIGNATURES = [
     ("chan_time_avg_start", ctypes.c_int, [ctypes.c_void_p]),
     ("chan_time_avg", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _I64, _D, _D]),
     ("chan_set_wall_bc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ChanWallBCC)]),
+    ("chan_diag_enable", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32,
+                                        _D, ctypes.c_double, ctypes.c_int32]),
+    ("chan_diag_read", ctypes.c_int, [ctypes.c_void_p, _D, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(ctypes.c_int64)]),
+    ("chan_fluctuation_q", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _D, _D]),
+    ("chan_q_criterion", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32), _D, _D, _D, _D, _D, _D, _D,
+                                        ctypes.c_int32]),
     ("chan_checkpoint_write", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_checkpoint_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_deck_read", ctypes.c_int, [ctypes.c_char_p, _I32, _D, _D, _D, _D, _D, _I64, ctypes.c_int32]),

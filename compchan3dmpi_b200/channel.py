@@ -188,6 +188,48 @@ class Channel:
             c.x1 = _lib.dptr(x1)
         self._check(self.L.chan_set_wall_bc(self._h, int(wall), ctypes.byref(c)))
 
+    def diag_enable(self, planes=(5, 10, 70, 100, 125), every: int = 10, x3q=None, x2end=None,
+                    capacity: int = 4096):
+        """Diagnostics series of main_v1.9.f90:799-906 every ``every`` steps, kept on
+        the device (0 turns it off).  x3q / x2end: the coordinates the reference
+        holds when it writes the series (after a restart, the deck's F10.6
+        columns); defaults: the mesh x3 and x2(nP2) accumulated from Ly."""
+        from .mesh import periodic_coords
+        pl = (ctypes.c_int32 * max(1, len(planes)))(*[int(p) for p in planes])
+        if x2end is None:
+            x2end = float(periodic_coords(self.nP[1], self.params.Ly)[-1])
+        z = None if x3q is None else np.ascontiguousarray(x3q, dtype=np.float64)
+        self._diag_np = len(planes)
+        self._check(self.L.chan_diag_enable(self._h, pl, len(planes), int(every),
+                                            None if z is None else _lib.dptr(z), float(x2end), int(capacity)))
+
+    def diag_read(self):
+        """Drain the device series: dict with nstep, time, ke (n,), rho_b, u_b,
+        rhou_b (n, nplanes) and lost (records the ring overwrote)."""
+        n = ctypes.c_int32(); lost = ctypes.c_int64()
+        self._check(self.L.chan_diag_read(self._h, None, 0, ctypes.byref(n), ctypes.byref(lost)))
+        npl = getattr(self, "_diag_np", 0)
+        rec = np.zeros((max(n.value, 1), 3 + 3 * npl))
+        self._check(self.L.chan_diag_read(self._h, _lib.dptr(rec), rec.shape[0], ctypes.byref(n),
+                                          ctypes.byref(lost)))
+        rec = rec[:n.value]
+        return {"nstep": rec[:, 0].astype(np.int64), "time": rec[:, 1], "ke": rec[:, 2],
+                "rho_b": rec[:, 3:3 + npl], "u_b": rec[:, 3 + npl:3 + 2 * npl],
+                "rhou_b": rec[:, 3 + 2 * npl:3 + 3 * npl], "lost": lost.value}
+
+    def fluctuation_q(self, mean, x1=None, x2=None, x3=None, want_fluc=True, want_q=True):
+        """(fluc, Q) of the current state on the device: fluc.f90:63-69 and
+        qInvariant.f90:26-81.  mean is (7, nP3); either output may be skipped."""
+        m = np.ascontiguousarray(mean, dtype=np.float64)
+        assert m.shape == (7, self.nP[2])
+        fl = np.empty(self.shape) if want_fluc else None
+        q = np.empty(self.shape[1:]) if want_q else None
+        cs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x1, x2, x3)]
+        self._check(self.L.chan_fluctuation_q(self._h, _lib.dptr(m), *[None if a is None else _lib.dptr(a) for a in cs],
+                                              None if fl is None else _lib.dptr(fl),
+                                              None if q is None else _lib.dptr(q)))
+        return fl, q
+
     def set_forcing(self, tauL: float, tauU: float, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         self._check(self.L.chan_set_forcing(self._h, float(tauL), float(tauU), _lib.dptr(rb)))
@@ -241,6 +283,21 @@ class Channel:
 
     def device_bytes(self) -> int:
         return int(self.L.chan_device_bytes(self._h))
+
+
+def q_criterion(u, v, w, x1, x2, x3, device: int = 0):
+    """Q-criterion (qInvariant.f90:26-81) of host velocity arrays (nP3, nP2, nP1) on a GPU."""
+    L = _lib.load()
+    u, v, w = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w))
+    n3, n2, n1 = u.shape
+    x1, x2, x3 = (np.ascontiguousarray(a, dtype=np.float64) for a in (x1, x2, x3))
+    Q = np.empty_like(u)
+    nP = (ctypes.c_int32 * 3)(n1, n2, n3)
+    r = L.chan_q_criterion(nP, _lib.dptr(u), _lib.dptr(v), _lib.dptr(w), _lib.dptr(x1), _lib.dptr(x2),
+                           _lib.dptr(x3), _lib.dptr(Q), int(device))
+    if r != 0:
+        raise ChanError(r, L.chan_last_error(None).decode())
+    return Q
 
 
 def version() -> str:

@@ -950,6 +950,161 @@ __global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const d
 }
 
 // ---------------------------------------------------------------------------
+// Diagnostics series (main_v1.9.f90:799-906), every `every` steps:
+//   KE = sum over all stored points of (u^2+v^2)+w^2, divided by nP1*nP2*nP3;
+//   bulk rho, u and rho*u through the x-planes i = plane(n): over the cells
+//   j=1..nP2-1, k=1..nP3-1 the mean of the four corner values times
+//   dAyz = dy*(x3(k+1)-x3(k)), summed and divided by Ayz = x3(nP3)*x2(nP2).
+// A plane outside 3..nP1-2 gives 0 (the single-rank form of the reference's
+// plane(i) > bn(1) .and. plane(i) < en(1) test).  Record layout:
+//   [nstep, time, KE, rho_b[np], U_b[np], rhoU_b[np]]
+// nstep is -1 when a blow-up stopped the run before that step's diagnostics.
+constexpr int kDiagMaxPlanes = 8;
+
+struct DiagParams {
+    int nplanes;
+    int planes[kDiagMaxPlanes];
+    const double *x3q;   // x3 as the diagnostics see it (the deck's F10.6 column after a restart)
+    double dy, Ayz;
+    double *part;        // nP3 per-plane KE sums
+};
+
+__global__ void __launch_bounds__(kStatThreads) k_diag_ke(const KParams P, const double *q, const DiagParams D)
+{
+    __shared__ double red[kStatThreads / 32];
+    const int n1 = P.n1, n2 = P.n2;
+    const int k = blockIdx.x + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (frozen(P.status, P.step + 1)) return;
+    double acc = 0.0;
+    const int np = n1 * n2;
+    for (int p = tid; p < np; p += kStatThreads) {
+        const int jj = p / n1, ii = p - jj * n1;
+        double x[7];
+        ref_var(P, q, ii + 1, jj + 1, k, x);
+        acc += (x[1] * x[1] + x[2] * x[2]) + x[3] * x[3];
+    }
+    const double s = warp_sum(acc);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kStatThreads / 32; w++) t += red[w];
+        D.part[k - 1] = t;
+    }
+}
+
+// block 0: KE from the per-plane sums; block 1+n*np+m: quantity n at plane m
+__global__ void __launch_bounds__(kStatThreads) k_diag_fin(const KParams P, const double *q, const DiagParams D,
+                                                           double *rec, double time)
+{
+    __shared__ double red[kStatThreads / 32];
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (frozen(P.status, P.step + 1)) {
+        if (b == 0 && tid == 0) rec[0] = -1.0;
+        return;
+    }
+    if (b == 0) {
+        if (tid == 0) {
+            double t = 0.0;
+            for (int k = 0; k < n3; k++) t += D.part[k];
+            rec[0] = (double)P.step;
+            rec[1] = time;
+            rec[2] = t / ((double)n1 * (double)n2 * (double)n3);
+        }
+        return;
+    }
+    const int qn = (b - 1) / D.nplanes, m = (b - 1) % D.nplanes;
+    const int ip = D.planes[m];
+    double acc = 0.0;
+    if (ip > 2 && ip < n1 - 1) {
+        const int nj = n2 - 1, ncell = (n2 - 1) * (n3 - 1);
+        for (int c = tid; c < ncell; c += kStatThreads) {
+            const int j = 1 + c % nj, k = 1 + c / nj;
+            double a[7], bb[7], cc[7], d[7];
+            ref_var(P, q, ip, j, k, a);
+            ref_var(P, q, ip, j + 1, k, bb);
+            ref_var(P, q, ip, j, k + 1, cc);
+            ref_var(P, q, ip, j + 1, k + 1, d);
+            double f0, f1, f2, f3;
+            if (qn == 0) { f0 = a[0]; f1 = bb[0]; f2 = cc[0]; f3 = d[0]; }
+            else if (qn == 1) { f0 = a[1]; f1 = bb[1]; f2 = cc[1]; f3 = d[1]; }
+            else { f0 = a[0] * a[1]; f1 = bb[0] * bb[1]; f2 = cc[0] * cc[1]; f3 = d[0] * d[1]; }
+            const double dAyz = D.dy * (D.x3q[k] - D.x3q[k - 1]);
+            acc += (0.25 * (((f0 + f1) + f2) + f3)) * dAyz;
+        }
+    }
+    const double s = warp_sum(acc);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kStatThreads / 32; w++) t += red[w];
+        rec[3 + qn * D.nplanes + m] = t / D.Ayz;
+    }
+}
+
+// fluctuation field var(i,j,k,:) - mean(k,:) (fluc.f90:63-69), in place on a
+// [7][N] device copy of var
+__global__ void k_fluctuation(double *var, const double *mean, int n1, int n2, int n3)
+{
+    const long long N = (long long)n1 * n2 * n3;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(p / ((long long)n1 * n2));
+#pragma unroll
+        for (int m = 0; m < 7; m++) var[(size_t)m * N + p] -= mean[(size_t)m * n3 + k];
+    }
+}
+
+// Q-criterion of a velocity field (qInvariant.f90:26-81): central differences
+// on the non-uniform coordinates x, y, z; Q = (P^2 - sum S^2 + sum R^2)/2 with
+// P = -trace(J), S and R the symmetric and antisymmetric parts of J.  Points
+// on the box faces get 0.  u, v, w and Q are [k][j][i].
+__global__ void k_qcrit(int n1, int n2, int n3, const double *u, const double *v, const double *w,
+                        const double *x, const double *y, const double *z, double *Q)
+{
+    const long long N = (long long)n1 * n2 * n3;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % n1);
+        const int j = (int)((p / n1) % n2);
+        const int k = (int)(p / ((long long)n1 * n2));
+        if (i == 0 || i == n1 - 1 || j == 0 || j == n2 - 1 || k == 0 || k == n3 - 1) {
+            Q[p] = 0.0;
+            continue;
+        }
+        const long long si = 1, sj = n1, sk = (long long)n1 * n2;
+        const double dx1 = x[i + 1] - x[i], dx2 = x[i] - x[i - 1];
+        const double dy1 = y[j + 1] - y[j], dy2 = y[j] - y[j - 1];
+        const double dz1 = z[k + 1] - z[k], dz2 = z[k] - z[k - 1];
+        const double *U[3] = {u, v, w};
+        double J[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double *f = U[c];
+            const double f0 = f[p];
+            J[c][0] = ((dx2 / dx1) * (f[p + si] - f0) + (dx1 / dx2) * (f0 - f[p - si])) / (dx1 + dx2);
+            J[c][1] = ((dy2 / dy1) * (f[p + sj] - f0) + (dy1 / dy2) * (f0 - f[p - sj])) / (dy1 + dy2);
+            J[c][2] = ((dz2 / dz1) * (f[p + sk] - f0) + (dz1 / dz2) * (f0 - f[p - sk])) / (dz1 + dz2);
+        }
+        // sum(S**2) and sum(-R**2) in column-major order
+        double as1 = 0.0, as2 = 0.0;
+#pragma unroll
+        for (int cj = 0; cj < 3; cj++)
+#pragma unroll
+            for (int ci = 0; ci < 3; ci++) {
+                const double sv = ci == cj ? J[ci][ci] : 0.5 * (J[ci][cj] + J[cj][ci]);
+                const double rv = ci == cj ? 0.0 : 0.5 * (J[ci][cj] - J[cj][ci]);
+                as1 += sv * sv;
+                as2 += -(rv * rv);
+            }
+        const double P_ = -((J[0][0] + J[1][1]) + J[2][2]);
+        Q[p] = 0.5 * ((P_ * P_ - as1) - as2);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Upload: var(1:nP1,1:nP2,1:nP3,1:7) (device copy, [m][k][j][i]) -> state.
 // initSolV (main_v1.9.f90:284-294): Q = rho*(1,u,v,w,E) at every point.
 __global__ void k_upload(const KParams P, const double *var, double *qa, double *qb, double *qc, double *cs)

@@ -62,6 +62,14 @@ struct chan_ctx {
     std::vector<ProfPair> prof_pairs;
     std::vector<cudaEvent_t> ev_pool;
     size_t dev_bytes = 0;
+    std::vector<double> hx3;      // x3 given to chan_init
+    // diagnostics series (allocated by chan_diag_enable)
+    int diag_every = 0, diag_cap = 0, diag_reclen = 0;
+    long long diag_count = 0;     // records written since the last chan_diag_read
+    double *diag_rec = nullptr, *diag_part = nullptr, *diag_x3 = nullptr;
+    chan::DiagParams dp{};
+    // fluctuation / Q-criterion buffers (allocated on first use)
+    double *dq = nullptr, *dxyz = nullptr;
 };
 
 namespace {
@@ -201,6 +209,19 @@ int launch_stats(chan_ctx *c, long long step, int moments, int tau)
     return CHAN_OK;
 }
 
+int launch_diag(chan_ctx *c, long long step, double time)
+{
+    c->kp.step = step;
+    double *rec = c->diag_rec + (size_t)(c->diag_count % c->diag_cap) * c->diag_reclen;
+    chan::k_diag_ke<<<c->n3, chan::kStatThreads, 0, c->stream>>>(c->kp, c->q[c->cur], c->dp);
+    CK(c, cudaGetLastError());
+    chan::k_diag_fin<<<1 + 3 * c->dp.nplanes, chan::kStatThreads, 0, c->stream>>>(c->kp, c->q[c->cur], c->dp, rec,
+                                                                                   time);
+    CK(c, cudaGetLastError());
+    c->diag_count++;
+    return CHAN_OK;
+}
+
 // queue nsteps steps; host counters advance optimistically
 int enqueue_steps(chan_ctx *c, int nsteps)
 {
@@ -212,6 +233,10 @@ int enqueue_steps(chan_ctx *c, int nsteps)
         }
         c->nstep = step;
         c->time = c->time + c->p.dt;
+        if (c->diag_every > 0 && step % c->diag_every == 0) {
+            int r = launch_diag(c, step, c->time);
+            if (r) return r;
+        }
         if (c->p.istat > 0 && step % c->p.istat == 0) {
             int r = launch_stats(c, step, 1, 1);
             if (r) return r;
@@ -388,6 +413,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     c->plane = (long long)c->px * c->NJ;
     c->vol = c->plane * (n3 + 2);
     c->nstage = p->rk_scheme == CHAN_RK3 ? 3 : 2;
+    c->hx3.assign(x3, x3 + n3);
 
     int r;
     for (int b = 0; b < 3; b++)
@@ -902,6 +928,164 @@ int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1
     return CHAN_OK;
 }
 
+int chan_diag_enable(chan_ctx *c, const int32_t *planes, int32_t nplanes, int32_t every, const double *x3q,
+                     double x2end, int32_t capacity)
+{
+    if (!c) return CHAN_EINVAL;
+    if (every < 0 || nplanes < 0 || nplanes > CHAN_DIAG_MAX_PLANES || (nplanes > 0 && !planes) || capacity < 0) {
+        c->err = "chan_diag_enable: bad arguments";
+        return CHAN_EINVAL;
+    }
+    CK(c, cudaSetDevice(c->dev));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (every == 0) { c->diag_every = 0; c->diag_count = 0; return CHAN_OK; }
+    if (capacity < 1) { c->err = "chan_diag_enable: capacity must be >= 1"; return CHAN_EINVAL; }
+    if (!(x2end > 0)) { c->err = "chan_diag_enable: x2end must be > 0"; return CHAN_EINVAL; }
+    const int n3 = c->n3;
+    const double *z = x3q ? x3q : c->hx3.data();
+    if (!(z[n3 - 1] > 0)) { c->err = "chan_diag_enable: x3(nP3) must be > 0"; return CHAN_EINVAL; }
+    if (c->diag_rec) { cudaFree(c->diag_rec); c->diag_rec = nullptr; }
+    if (!c->diag_part) {
+        CK(c, cudaMalloc((void **)&c->diag_part, (size_t)n3 * sizeof(double)));
+        CK(c, cudaMalloc((void **)&c->diag_x3, (size_t)n3 * sizeof(double)));
+        c->dev_bytes += 2 * (size_t)n3 * sizeof(double);
+    }
+    const int reclen = 3 + 3 * nplanes;
+    CK(c, cudaMalloc((void **)&c->diag_rec, (size_t)capacity * reclen * sizeof(double)));
+    CK(c, cudaMemcpy(c->diag_x3, z, (size_t)n3 * sizeof(double), cudaMemcpyHostToDevice));
+    chan::DiagParams &D = c->dp;
+    D.nplanes = nplanes;
+    for (int m = 0; m < chan::kDiagMaxPlanes; m++) D.planes[m] = m < nplanes ? planes[m] : 0;
+    D.x3q = c->diag_x3;
+    D.dy = c->p.Ly / (double)(c->n2 - 1);
+    D.Ayz = z[n3 - 1] * x2end;
+    D.part = c->diag_part;
+    c->diag_every = every;
+    c->diag_cap = capacity;
+    c->diag_reclen = reclen;
+    c->diag_count = 0;
+    return CHAN_OK;
+}
+
+int chan_diag_read(chan_ctx *c, double *records, int32_t max_records, int32_t *nrecords, int64_t *lost)
+{
+    if (!c || !nrecords) return CHAN_EINVAL;
+    if (!c->diag_rec) { *nrecords = 0; if (lost) *lost = 0; return CHAN_OK; }
+    CK(c, cudaSetDevice(c->dev));
+    const long long avail = c->diag_count < c->diag_cap ? c->diag_count : c->diag_cap;
+    if (!records) { *nrecords = (int32_t)avail; if (lost) *lost = c->diag_count - avail; return CHAN_OK; }
+    if (max_records < avail) { c->err = "chan_diag_read: records buffer too small"; return CHAN_EINVAL; }
+    std::vector<double> ring((size_t)c->diag_cap * c->diag_reclen);
+    CK(c, cudaMemcpyAsync(ring.data(), c->diag_rec, ring.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    const long long first = c->diag_count - avail;  // index of the oldest record kept
+    int32_t n = 0;
+    for (long long r = first; r < c->diag_count; r++) {
+        const double *src = ring.data() + (size_t)(r % c->diag_cap) * c->diag_reclen;
+        if (src[0] < 0) continue;  // after a blow-up
+        memcpy(records + (size_t)n * c->diag_reclen, src, c->diag_reclen * sizeof(double));
+        n++;
+    }
+    *nrecords = n;
+    if (lost) *lost = first;
+    c->diag_count = 0;
+    return CHAN_OK;
+}
+
+namespace {
+int upload_coords(chan_ctx *c, const double *x1, const double *x2, const double *x3, double *dst)
+{
+    const int n1 = c->n1, n2 = c->n2, n3 = c->n3;
+    std::vector<double> h((size_t)n1 + n2 + n3);
+    for (int i = 0; i < n1; i++) h[i] = x1 ? x1[i] : 0.0;
+    if (!x1) {  // x1(1)=0, x1(i+1)=x1(i)+dx (v1.9/codes/comdata.f90:93-95)
+        const double dx = c->p.Lx / (double)(n1 - 1);
+        for (int i = 1; i < n1; i++) h[i] = h[i - 1] + dx;
+    }
+    for (int j = 0; j < n2; j++) h[n1 + j] = x2 ? x2[j] : 0.0;
+    if (!x2) {
+        const double dy = c->p.Ly / (double)(n2 - 1);
+        for (int j = 1; j < n2; j++) h[n1 + j] = h[n1 + j - 1] + dy;
+    }
+    for (int k = 0; k < n3; k++) h[n1 + n2 + k] = x3 ? x3[k] : c->hx3[k];
+    CK(c, cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+}  // namespace
+
+int chan_fluctuation_q(chan_ctx *c, const double *mean, const double *x1, const double *x2, const double *x3,
+                       double *fluc, double *qcrit)
+{
+    if (!c || !mean) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    const size_t N = (size_t)c->n1 * c->n2 * c->n3;
+    if (!c->dq) {
+        CK(c, cudaMalloc((void **)&c->dq, (N + 7 * (size_t)c->n3) * sizeof(double)));
+        CK(c, cudaMalloc((void **)&c->dxyz, ((size_t)c->n1 + c->n2 + c->n3) * sizeof(double)));
+        c->dev_bytes += (N + 7 * (size_t)c->n3 + c->n1 + c->n2 + c->n3) * sizeof(double);
+    }
+    double *dmean = c->dq + N;
+    int r = upload_coords(c, x1, x2, x3, c->dxyz);
+    if (r) return r;
+    CK(c, cudaMemcpyAsync(dmean, mean, 7 * (size_t)c->n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    chan::k_download<<<1184, 256, 0, c->stream>>>(c->kp, c->q[c->cur], c->dvar);
+    CK(c, cudaGetLastError());
+    chan::k_fluctuation<<<1184, 256, 0, c->stream>>>(c->dvar, dmean, c->n1, c->n2, c->n3);
+    CK(c, cudaGetLastError());
+    if (qcrit) {
+        chan::k_qcrit<<<1184, 256, 0, c->stream>>>(c->n1, c->n2, c->n3, c->dvar + N, c->dvar + 2 * N,
+                                                    c->dvar + 3 * N, c->dxyz, c->dxyz + c->n1,
+                                                    c->dxyz + c->n1 + c->n2, c->dq);
+        CK(c, cudaGetLastError());
+        CK(c, cudaMemcpyAsync(qcrit, c->dq, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (fluc) CK(c, cudaMemcpyAsync(fluc, c->dvar, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
+int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const double *w, const double *x1,
+                     const double *x2, const double *x3, double *qcrit, int32_t device)
+{
+    g_init_error.clear();
+    if (!nP || !u || !v || !w || !x1 || !x2 || !x3 || !qcrit) { g_init_error = "NULL argument"; return CHAN_EINVAL; }
+    const long long n1 = nP[0], n2 = nP[1], n3 = nP[2];
+    if (n1 < 1 || n2 < 1 || n3 < 1 || n1 * n2 * n3 > (1LL << 31)) { g_init_error = "bad nP"; return CHAN_EINVAL; }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { fail(nullptr, "cudaSetDevice", e); return CHAN_ECUDA; }
+    const size_t N = (size_t)(n1 * n2 * n3);
+    const size_t nc = (size_t)(n1 + n2 + n3);
+    double *d = nullptr;
+    int rc = CHAN_OK;
+    e = cudaMalloc((void **)&d, (4 * N + nc) * sizeof(double));
+    if (e != cudaSuccess) { fail(nullptr, "cudaMalloc", e); cudaSetDevice(prev); return CHAN_ENOMEM; }
+    cudaStream_t st = nullptr;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, u, N * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + N, v, N * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + 2 * N, w, N * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + 4 * N, x1, n1 * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + 4 * N + n1, x2, n2 * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + 4 * N + n1 + n2, x3, n3 * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        chan::k_qcrit<<<1184, 256, 0, st>>>((int)n1, (int)n2, (int)n3, d, d + N, d + 2 * N, d + 4 * N,
+                                            d + 4 * N + n1, d + 4 * N + n1 + n2, d + 3 * N);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(qcrit, d + 3 * N, N * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail(nullptr, "chan_q_criterion", e);
+    if (st) cudaStreamDestroy(st);
+    cudaFree(d);
+    cudaSetDevice(prev);
+    return rc;
+}
+
 void chan_free(chan_ctx *c)
 {
     if (!c) return;
@@ -921,6 +1105,11 @@ void chan_free(chan_ctx *c)
     }
     if (c->stat) cudaFree(c->stat);
     if (c->dvar) cudaFree(c->dvar);
+    if (c->diag_rec) cudaFree(c->diag_rec);
+    if (c->diag_part) cudaFree(c->diag_part);
+    if (c->diag_x3) cudaFree(c->diag_x3);
+    if (c->dq) cudaFree(c->dq);
+    if (c->dxyz) cudaFree(c->dxyz);
     if (c->status) cudaFree(c->status);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -137,3 +137,37 @@ def read_series(path, ncol, n3):
         times.append(nums[0])
         vals.append(np.array(nums[1:]).reshape(n3, ncol).T)
     return np.array(times), np.array(vals)
+
+
+# ------------------------------------------------------------ diagnostics series
+def _f15_7(x):
+    return f"{float(x):15.7f}"
+
+
+def append_diag_series(outdir, d):
+    """Append a diag_read() result to KE.dat (format 2(1X,F15.7)) and
+    rhobulk.dat, Ubulk.dat, massflow.dat (6(1X,F15.7)): time then one column
+    per plane (main_v1.9.f90:813-906)."""
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    with open(out / "KE.dat", "a") as f:
+        for t, ke in zip(d["time"], d["ke"]):
+            f.write(" " + _f15_7(t) + " " + _f15_7(ke) + "\n")
+    for name, key in (("rhobulk.dat", "rho_b"), ("Ubulk.dat", "u_b"), ("massflow.dat", "rhou_b")):
+        with open(out / name, "a") as f:
+            for t, row in zip(d["time"], d[key]):
+                f.write(" " + _f15_7(t) + "".join(" " + _f15_7(v) for v in row) + "\n")
+
+
+def write_q_invariant(path, x1, x2, x3, Q):
+    """qInvariant.dat as qInvariant.f90:84-95 writes it: list-directed header
+    lines, then x,y,z,Q records 3(1X,F10.6),1X,E22.15 with i fastest."""
+    from .deck import fmt_e22_15
+    n3, n2, n1 = Q.shape
+    lines = [' TITLE ="qInvariant"', ' Variables = "x","y","z","Q"',
+             f'ZONE i={n1:3d},j={n2:3d},k={n3:3d},DATAPACKING="POINT"']
+    for k in range(n3):
+        for j in range(n2):
+            for i in range(n1):
+                lines.append(f" {x1[i]:10.6f} {x2[j]:10.6f} {x3[k]:10.6f} " + fmt_e22_15(float(Q[k, j, i])))
+    Path(path).write_text("\n".join(lines) + "\n")

@@ -263,6 +263,50 @@ const char *chan_io_last_error(void);
 int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1, double *stat2, double *corr,
                              int32_t device);
 
+/* Diagnostics series (v1.9/codes/main_v1.9.f90:799-906), computed on the
+ * device inside chan_step every `every` steps (the reference: every 10) and
+ * kept in a device ring of `capacity` records until chan_diag_read:
+ *   KE      = sum over all points of u^2+v^2+w^2 / (nP1*nP2*nP3)    (KE.dat)
+ *   rho_b   = bulk density through each x-plane i = planes[m]    (rhobulk.dat)
+ *   U_b     = bulk velocity                                         (Ubulk.dat)
+ *   rhoU_b  = mass flow                                          (massflow.dat)
+ * Bulk values sum, over the cells j=1..nP2-1, k=1..nP3-1 of the plane, the
+ * mean of the four corner values times dy*(x3q(k+1)-x3q(k)), then divide by
+ * x3q(nP3)*x2end.  A plane outside 3..nP1-2 reports 0, as the reference's
+ * single-rank test does.  x3q (nP3 values) and x2end are the coordinates the
+ * reference holds when it writes these series: after a restart, the deck's
+ * F10.6 columns (x3q NULL: the x3 given to chan_init).  The reference uses
+ * planes = {5, 10, 70, 100, 125}.
+ * Record layout (3 + 3*nplanes doubles):
+ *   [nstep, time, KE, rho_b[nplanes], U_b[nplanes], rhoU_b[nplanes]]
+ * chan_diag_enable with every = 0 turns the series off.  chan_diag_read waits
+ * for queued work, copies the records in step order (none after a blow-up)
+ * and empties the ring; records is NULL to query the count only.  *lost counts
+ * the records the ring overwrote. */
+#define CHAN_DIAG_MAX_PLANES 8
+int chan_diag_enable(chan_ctx *c, const int32_t *planes, int32_t nplanes, int32_t every, const double *x3q,
+                     double x2end, int32_t capacity);
+int chan_diag_read(chan_ctx *c, double *records, int32_t max_records, int32_t *nrecords, int64_t *lost);
+
+/* Fluctuation field and Q-criterion of the context's current state, on the
+ * device.  fluc = var(i,j,k,:) - mean(k,:) as v1.9/codes/fluc.f90:63-69
+ * forms it (mean: 7*nP3 doubles stored [p][k], e.g. the time-averaged
+ * stat1Spc); qcrit = Q of the fluctuating velocity (u',v',w') as
+ * v1.9_strat/v1.9_st1/codes/qInvariant.f90:26-81 computes it:
+ * non-uniform central differences on x1, x2, x3, S and R the symmetric and
+ * antisymmetric parts of the velocity gradient, Q = (P^2 - sum S^2 + sum R^2)/2
+ * with P = -trace; 0 on the box faces.  x1, x2, x3 may be NULL (the
+ * context's coordinates: x1, x2 accumulated from Lx, Ly; x3 given to
+ * chan_init).  fluc (7*N, var layout) and qcrit (N) may be NULL. */
+int chan_fluctuation_q(chan_ctx *c, const double *mean, const double *x1, const double *x2, const double *x3,
+                       double *fluc, double *qcrit);
+
+/* The same Q-criterion for host velocity arrays u, v, w (nP1*nP2*nP3 each,
+ * i fastest) on GPU `device`, without a context.  It allocates and frees
+ * its device buffers.  Errors: chan_last_error(NULL). */
+int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const double *w, const double *x1,
+                     const double *x2, const double *x3, double *qcrit, int32_t device);
+
 /* Free device memory and the context.  NULL is allowed. */
 void chan_free(chan_ctx *c);
 

@@ -824,3 +824,100 @@ void orc_set_num_threads(int n)
     (void)n;
 #endif
 }
+
+/* ---- diagnostics series of a field var(1:nP1,1:nP2,1:nP3,1:7) (i fastest):
+ * main_v1.9.f90:799-906 on one rank (bs=1, es=nP, bn(1)=2, en(1)=nP1-1).
+ * out = [KE, rho_b[np], U_b[np], rhoU_b[np]]; x3q are the x3 the reference
+ * holds, x2end its x2(nP2), dy = Ly/(nP2-1). */
+#define FV(m, i, j, k) var[(size_t)((m) - 1) * N + (((size_t)(k) - 1) * n2 + ((size_t)(j) - 1)) * n1 + ((size_t)(i) - 1)]
+void orc_diagnostics(const double *var, const int *nP, const int *planes, int np, const double *x3q, double dy,
+                     double x2end, double *out)
+{
+    const int n1 = nP[0], n2 = nP[1], n3 = nP[2];
+    const size_t N = (size_t)n1 * n2 * n3;
+    const double quar = 0.25, two = 2.0;
+    double tmpR1 = 0.0, Ayz;
+    int i, j, k, p, q;
+    (void)two;
+    /* KE: main19:801-817 */
+    for (k = 1; k <= n3; k++)
+        for (j = 1; j <= n2; j++)
+            for (i = 1; i <= n1; i++) {
+                const double u = FV(2, i, j, k), v = FV(3, i, j, k), w = FV(4, i, j, k);
+                tmpR1 = tmpR1 + ((u * u + v * v) + w * w);
+            }
+    out[0] = tmpR1 / ((double)n1 * (double)n2 * (double)n3);
+    /* bulk rho, U, rho*U: main19:821-906 */
+    Ayz = x3q[n3 - 1] * x2end;
+    for (q = 0; q < 3; q++)
+        for (p = 0; p < np; p++) {
+            const int ip = planes[p];
+            tmpR1 = 0.0;
+            if (ip > 2 && ip < n1 - 1) {
+                for (k = 1; k <= n3 - 1; k++)
+                    for (j = 1; j <= n2 - 1; j++) {
+                        const double dAyz = dy * (x3q[k] - x3q[k - 1]);
+                        double a, b, c, d;
+                        if (q == 0) {
+                            a = FV(1, ip, j, k); b = FV(1, ip, j + 1, k); c = FV(1, ip, j, k + 1); d = FV(1, ip, j + 1, k + 1);
+                        } else if (q == 1) {
+                            a = FV(2, ip, j, k); b = FV(2, ip, j + 1, k); c = FV(2, ip, j, k + 1); d = FV(2, ip, j + 1, k + 1);
+                        } else {
+                            a = FV(1, ip, j, k) * FV(2, ip, j, k);
+                            b = FV(1, ip, j + 1, k) * FV(2, ip, j + 1, k);
+                            c = FV(1, ip, j, k + 1) * FV(2, ip, j, k + 1);
+                            d = FV(1, ip, j + 1, k + 1) * FV(2, ip, j + 1, k + 1);
+                        }
+                        tmpR1 = tmpR1 + quar * (((a + b) + c) + d) * dAyz;
+                    }
+            }
+            out[1 + q * np + p] = tmpR1 / Ayz;
+        }
+}
+#undef FV
+
+/* ---- Q-criterion: v1.9_strat/v1.9_st1/codes/qInvariant.f90:26-81.
+ * u,v,w,Q are nP1*nP2*nP3 (i fastest); box faces get 0. */
+void orc_qcrit(const int *nP, const double *u, const double *v, const double *w, const double *x, const double *y,
+               const double *z, double *Q)
+{
+    const int n1 = nP[0], n2 = nP[1], n3 = nP[2];
+    const double haf = 0.5;
+    const double *Ut[3] = {u, v, w};
+    int i, j, k;
+    memset(Q, 0, sizeof(double) * (size_t)n1 * n2 * n3);
+    for (k = 2; k <= n3 - 1; k++)
+        for (j = 2; j <= n2 - 1; j++)
+            for (i = 2; i <= n1 - 1; i++) {
+                const size_t c0 = (((size_t)k - 1) * n2 + (j - 1)) * n1 + (i - 1);
+                const size_t si = 1, sj = (size_t)n1, sk = (size_t)n1 * n2;
+                double dx[3][2], Jt[3][3], S[3][3], R[3][3], As1, As2, P;
+                int jc, a, b;
+                dx[0][0] = x[i] - x[i - 1]; dx[1][0] = y[j] - y[j - 1]; dx[2][0] = z[k] - z[k - 1];
+                dx[0][1] = x[i - 1] - x[i - 2]; dx[1][1] = y[j - 1] - y[j - 2]; dx[2][1] = z[k - 1] - z[k - 2];
+                for (jc = 0; jc < 3; jc++) {
+                    const double *U = Ut[jc];
+                    Jt[jc][0] = ((dx[0][1] / dx[0][0]) * (U[c0 + si] - U[c0]) + (dx[0][0] / dx[0][1]) * (U[c0] - U[c0 - si]))
+                                / (dx[0][0] + dx[0][1]);
+                    Jt[jc][1] = ((dx[1][1] / dx[1][0]) * (U[c0 + sj] - U[c0]) + (dx[1][0] / dx[1][1]) * (U[c0] - U[c0 - sj]))
+                                / (dx[1][0] + dx[1][1]);
+                    Jt[jc][2] = ((dx[2][1] / dx[2][0]) * (U[c0 + sk] - U[c0]) + (dx[2][0] / dx[2][1]) * (U[c0] - U[c0 - sk]))
+                                / (dx[2][0] + dx[2][1]);
+                }
+                S[0][0] = Jt[0][0]; S[0][1] = haf * (Jt[0][1] + Jt[1][0]); S[0][2] = haf * (Jt[0][2] + Jt[2][0]);
+                S[1][0] = haf * (Jt[1][0] + Jt[0][1]); S[1][1] = Jt[1][1]; S[1][2] = haf * (Jt[2][1] + Jt[1][2]);
+                S[2][0] = haf * (Jt[2][0] + Jt[0][2]); S[2][1] = haf * (Jt[2][1] + Jt[1][2]); S[2][2] = Jt[2][2];
+                R[0][0] = 0.0; R[0][1] = haf * (Jt[0][1] - Jt[1][0]); R[0][2] = haf * (Jt[0][2] - Jt[2][0]);
+                R[1][0] = haf * (Jt[1][0] - Jt[0][1]); R[1][1] = 0.0; R[1][2] = haf * (Jt[1][2] - Jt[2][1]);
+                R[2][0] = haf * (Jt[2][0] - Jt[0][2]); R[2][1] = haf * (Jt[2][1] - Jt[1][2]); R[2][2] = 0.0;
+                /* sum(S**2.0), sum(-R**2.0) in array-element (column-major) order */
+                As1 = 0.0; As2 = 0.0;
+                for (b = 0; b < 3; b++)
+                    for (a = 0; a < 3; a++) {
+                        As1 = As1 + S[a][b] * S[a][b];
+                        As2 = As2 + (-(R[a][b] * R[a][b]));
+                    }
+                P = -((S[0][0] + S[1][1]) + S[2][2]);
+                Q[c0] = haf * ((P * P - As1) - As2);
+            }
+}

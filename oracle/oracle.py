@@ -69,6 +69,8 @@ def lib():
         L.orc_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D]
         L.orc_set_wall_bc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, _D, ctypes.c_void_p, _D, _D]
+        L.orc_diagnostics.argtypes = [_D, _I, _I, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, _D]
+        L.orc_qcrit.argtypes = [_I, _D, _D, _D, _D, _D, _D, _D]
         L.orc_nstep.argtypes = [ctypes.c_void_p]
         L.orc_nstep.restype = ctypes.c_long
         L.orc_time.argtypes = [ctypes.c_void_p]
@@ -205,6 +207,35 @@ class Oracle:
         ijk = (ctypes.c_int * 3)()
         f = lib().orc_blown(self._h, ijk)
         return f, tuple(ijk)
+
+
+def diagnostics(var, planes, x3q, dy, x2end):
+    """[KE, rho_b[np], U_b[np], rhoU_b[np]] of var (7, nP3, nP2, nP1):
+    main_v1.9.f90:799-906 on one rank."""
+    v = np.ascontiguousarray(var, dtype=np.float64)
+    _, n3, n2, n1 = v.shape
+    nP = (ctypes.c_int * 3)(n1, n2, n3)
+    pl = (ctypes.c_int * max(1, len(planes)))(*[int(p) for p in planes])
+    z = np.ascontiguousarray(x3q, dtype=np.float64)
+    out = np.zeros(1 + 3 * len(planes))
+    lib().orc_diagnostics(_dp(v), nP, pl, len(planes), _dp(z), float(dy), float(x2end), _dp(out))
+    return out
+
+
+def fluctuation(var, mean):
+    """var(i,j,k,:) - mean(k,:) (fluc.f90:63-69); mean is (7, nP3)."""
+    return np.asarray(var, dtype=np.float64) - np.asarray(mean, dtype=np.float64)[:, :, None, None]
+
+
+def qcrit(u, v, w, x, y, z):
+    """Q-criterion of qInvariant.f90:26-81; u, v, w are (nP3, nP2, nP1)."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    n3, n2, n1 = u.shape
+    v = np.ascontiguousarray(v, dtype=np.float64); w = np.ascontiguousarray(w, dtype=np.float64)
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    Q = np.empty_like(u)
+    lib().orc_qcrit((ctypes.c_int * 3)(n1, n2, n3), _dp(u), _dp(v), _dp(w), _dp(x), _dp(y), _dp(z), _dp(Q))
+    return Q
 
 
 def num_threads() -> int:
