@@ -62,6 +62,7 @@ struct KParams {
     // forcing / stats
     double *stat;         // stat1[7*n3] | stat2[7*n3] | corr[9*n3] | tau[2]
     double *tacc;         // running sums of the same 23*n3+2 numbers over statistics steps
+    double *hwt;          // [4][nP2+2][px] hD on the top wall plane, staged by the last k-chunk
     DevStatus *status;
     // physics
     double invRe, ggM, ggMh, gM2, inv_gM2, kq, two3rd;
@@ -238,15 +239,11 @@ __device__ __forceinline__ void visc_fxy(const KParams &P, const Slot &s, const 
     g[3] = -(kqm * Ty) + P.ggM * ((-(u0 * t12) + v0 * g3) + w0 * g4);
 }
 
-// hD at the thread's own column; z-derivatives supplied by the caller
-template <int BX>
-__device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double mu, double pr, int b,
-                                        double uz, double vz, double wz, double Tz, double h[4])
+// hD from its in-plane derivatives, point values and z-derivatives
+__device__ __forceinline__ void visc_fz_vals(const KParams &P, double ux, double vy, double wx, double wy, double u,
+                                             double v, double w, double mu, double pr, double uz, double vz,
+                                             double wz, double Tz, double h[4])
 {
-    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
-    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
-    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
-    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
     const double mr = mu * P.invRe;
     const double div = (ux + vy) + wz;
     const double h2 = -(mr * (wx + uz));
@@ -255,7 +252,28 @@ __device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double 
     h[0] = h2;
     h[1] = h3;
     h[2] = h4;
-    h[3] = -((P.kq * mu) * Tz) + P.ggM * ((s.U[b] * h2 + s.V[b] * h3) + s.W[b] * h4);
+    h[3] = -((P.kq * mu) * Tz) + P.ggM * ((u * h2 + v * h3) + w * h4);
+}
+
+// hD at the thread's own column; z-derivatives supplied by the caller
+template <int BX>
+__device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double mu, double pr, int b,
+                                        double uz, double vz, double wz, double Tz, double h[4])
+{
+    visc_fz_vals(P, (s.U[b + 1] - s.U[b - 1]) * P.hdx, (s.V[b + BX] - s.V[b - BX]) * P.hdy,
+                 (s.W[b + 1] - s.W[b - 1]) * P.hdx, (s.W[b + BX] - s.W[b - BX]) * P.hdy, s.U[b], s.V[b], s.W[b],
+                 mu, pr, uz, vz, wz, Tz, h);
+}
+
+// periodic image of index i in 0..n+1 (duplicate-point period n-2):
+// q(0)=q(n-2), q(1)=q(n-1), q(n)=q(2), q(n+1)=q(3)
+__device__ __forceinline__ int wrap_idx(int i, int n)
+{
+    if (i == 0) return n - 2;
+    if (i == 1) return n - 1;
+    if (i == n) return 2;
+    if (i == n + 1) return 3;
+    return i;
 }
 
 // ---------------------------------------------------------------------------
@@ -385,7 +403,13 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         lo[l] = gj * P.px + gi;
     }
 
-    // fill the ring slots of plane m over the whole box
+    // fill the ring slots of plane m over the whole box.  A wall plane's box
+    // holds, at periodic duplicates and ghosts, the values of their image
+    // points: the viscous fluxes next to a wall read the wall only there, and
+    // the reference's flux at a duplicate column or row is the exchanged flux
+    // of its image (whose wall values may differ from the duplicate's own
+    // under a non-periodic wall BC).  hD on a wall plane reads the wall's own
+    // values from memory instead (hflux_wall).
     auto load_plane = [&](int m) {
         const Slot s = slot(m);
         double *MU = smu(m), *PR = spr(m);
@@ -404,7 +428,8 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             }
             double u, vv, w, T, mu, pr;
             if (wall) {
-                const long long wo = lo[l];
+                const int bj = p / BX, bi = p - bj * BX;
+                const long long wo = (long long)wrap_idx(j0 - 2 + bj, n2) * P.px + wrap_idx(i0 - 2 + bi, n1);
                 u = W[1 * plane + wo];
                 vv = W[2 * plane + wo];
                 w = W[3 * plane + wo];
@@ -438,21 +463,30 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         }
     };
 
-    // hD at the own column of plane m (in ring); dz from (m-1, m+1) values
+    // hD at the own column of interior plane m (in ring); dz from (m-1, m+1) values
     auto hflux = [&](int m, double um, double vm, double wm, double Tm, double up, double vp, double wp_,
                      double Tp, double h[4]) {
         const Slot s = slot(m);
-        double sc;
-        if (m == 1) {
-            // one-sided at the bottom wall: (q(2)-q(1))/dz1 ; "m-1" slot is the wall itself
-            sc = P.inv_dz1;
-        } else if (m == n3) {
-            sc = P.inv_dzN;
-        } else {
-            sc = P.czh[m];
-        }
+        const double sc = P.czh[m];
         visc_fz<BX>(P, s, smu(m)[bc], spr(m)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
                     (Tp - Tm) * sc, h);
+    };
+    // hD at the own column of wall plane m, from the wall's own values in
+    // memory; one-sided dz against the interior neighbour values (ui..Ti):
+    // (q(2)-q(1))/dz1 at the bottom, (q(nP3)-q(nP3-1))/dzN at the top.  The
+    // pressure is the pressure-BC state.
+    auto hflux_wall = [&](int m, double ui, double vi, double wi, double Ti, double h[4]) {
+        const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane + colo;
+        const long long px = P.px;
+        const double u0 = W[plane], v0 = W[2 * plane], w0 = W[3 * plane], T0 = W[5 * plane];
+        const double sc = m == 1 ? P.inv_dz1 : P.inv_dzN;
+        const double ux = (W[plane + 1] - W[plane - 1]) * P.hdx;
+        const double vy = (W[2 * plane + px] - W[2 * plane - px]) * P.hdy;
+        const double wx = (W[3 * plane + 1] - W[3 * plane - 1]) * P.hdx;
+        const double wy = (W[3 * plane + px] - W[3 * plane - px]) * P.hdy;
+        const double uz = (m == 1 ? ui - u0 : u0 - ui) * sc, vz = (m == 1 ? vi - v0 : v0 - vi) * sc;
+        const double wz = (m == 1 ? wi - w0 : w0 - wi) * sc, Tz = (m == 1 ? Ti - T0 : T0 - Ti) * sc;
+        visc_fz_vals(P, ux, vy, wx, wy, u0, v0, w0, W[7 * plane], W[6 * plane], uz, vz, wz, Tz, h);
     };
 
     // ---------------- prologue: planes kb-1 and kb, hD(kb-1), hD(kb)
@@ -466,7 +500,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         if (col_ok) {
             // hD(kb-1)
             if (kb - 1 == 1) {
-                hflux(1, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                hflux_wall(1, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
             } else {
                 double q[5], u, v, w, T;
                 center(kb - 2, q, u, v, w, T);
@@ -482,6 +516,14 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 double u, v, w, T;
                 center(kb - 2, qm2, u, v, w, T);
                 wm2 = w;
+            }
+            // the last chunk stages hD of the top wall plane for its last plane
+            if (ke == n3 - 1) {
+                double q[5], u, v, w, T, h[4];
+                center(n3 - 1, q, u, v, w, T);
+                hflux_wall(n3, u, v, w, T, h);
+#pragma unroll
+                for (int c = 0; c < 4; c++) P.hwt[c * plane + colo] = h[c];
             }
 #pragma unroll
             for (int c = 0; c < 5; c++) qm1[c] = sq(kb - 1, c)[bc];
@@ -507,9 +549,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             const double czt = P.czh[t];
             const double *MU = smu(t), *PR = spr(t);
             if (col_ok) {
-                if (t + 1 == n3)
-                    hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], sp.U[bc], sp.V[bc], sp.W[bc], sp.T[bc], hp1);
-                else
+                if (t + 1 != n3)
                     hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 double f[4], g[4];
                 visc_fxy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f, g);
@@ -604,10 +644,12 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 }
                 const double czt = P.czh[t];
                 R[0] = R[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(t + 1, 0)[bc], qp2[0]);
+                const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
                     const double H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(t + 1, c)[bc], qp2[c]);
-                    const double H2 = (hp1[c - 1] - hm1[c - 1]) * czt;
+                    const double hp = top ? P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
+                    const double H2 = (hp - hm1[c - 1]) * czt;
                     R[c] = (R[c] + H1) + H2;
                 }
             }
@@ -1145,14 +1187,6 @@ __global__ void k_upload(const KParams P, const double *var, double *qa, double 
 // periodic images of Q for interior planes (the reference's initial share2P,
 // including corner images so every periodic read is consistent); and of the
 // wall planes' primitive ring i,j in {0, nP+1}
-__device__ __forceinline__ int wrap_idx(int i, int n)
-{
-    if (i == 0) return n - 2;
-    if (i == 1) return n - 1;
-    if (i == n) return 2;
-    if (i == n + 1) return 3;
-    return i;
-}
 
 __global__ void k_fill_ghosts(const KParams P, double *q)
 {

@@ -41,6 +41,7 @@ struct chan_ctx {
     chan::KParams kp{};
     double *q[3] = {nullptr, nullptr, nullptr};
     double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr, *tacc = nullptr;
+    double *hwt = nullptr;   // hD of the top wall plane, staged inside a stage
     unsigned char *wmask[2] = {nullptr, nullptr};  // wall-BC plug-in arrays (allocated on first use)
     double *wuv[2] = {nullptr, nullptr}, *wx1[2] = {nullptr, nullptr};
     long long tavg_samples = 0;  // statistics steps summed into tacc since chan_time_avg_start
@@ -420,7 +421,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
         if ((r = dalloc(c, &c->q[b], 5 * (size_t)c->vol))) { g_init_error = c->err; chan_free(c); return r; }
     if ((r = dalloc(c, &c->wp, 2 * 8 * (size_t)c->plane)) || (r = dalloc(c, &c->cs, (size_t)(n3 + 2) * 28)) ||
         (r = dalloc(c, &c->tabs, 4 * (size_t)(n3 + 2))) || (r = dalloc(c, &c->stat, 23 * (size_t)n3 + 2)) ||
-        (r = dalloc(c, &c->tacc, 23 * (size_t)n3 + 2)) ||
+        (r = dalloc(c, &c->tacc, 23 * (size_t)n3 + 2)) || (r = dalloc(c, &c->hwt, 4 * (size_t)c->plane)) ||
         (r = dalloc(c, &c->dvar, 7 * (size_t)n1 * n2 * n3))) {
         g_init_error = c->err;
         chan_free(c);
@@ -455,7 +456,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     k.plane = c->plane; k.vol = c->vol;
     k.wp = c->wp; k.cs = c->cs;
     k.czh = c->tabs; k.cz8 = c->tabs + (n3 + 2); k.cz12 = c->tabs + 2 * (n3 + 2); k.pez = c->tabs + 3 * (n3 + 2);
-    k.stat = c->stat; k.status = c->status; k.tacc = c->tacc; k.acc_on = 0;
+    k.stat = c->stat; k.status = c->status; k.tacc = c->tacc; k.acc_on = 0; k.hwt = c->hwt;
     k.invRe = 1.0 / Re;
     k.ggM = gama * (gama - 1) * (Mac * Mac);
     k.ggMh = k.ggM * 0.5;
@@ -1098,6 +1099,7 @@ void chan_free(chan_ctx *c)
     if (c->cs) cudaFree(c->cs);
     if (c->tabs) cudaFree(c->tabs);
     if (c->tacc) cudaFree(c->tacc);
+    if (c->hwt) cudaFree(c->hwt);
     for (int w = 0; w < 2; w++) {
         if (c->wmask[w]) cudaFree(c->wmask[w]);
         if (c->wuv[w]) cudaFree(c->wuv[w]);
