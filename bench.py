@@ -294,8 +294,8 @@ def run_ours(args):
         achieved = n_int * bpp / (stage_ms_max / 1e3) / 1e9
         peak, peak_kind = hbm_peak()
         traffic = measured_traffic(p, n_int)
-        # stage + wall-BC kernels per stage, plus the statistics kernel on its cadence
-        launches = K * 2 * stages + sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
+        # stage + wall-BC kernels per stage, plus the two statistics passes on their cadence
+        launches = K * 2 * stages + 2 * sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -15,7 +15,7 @@
 //                              statistics sum them; kept only for that.
 //
 // One RK stage = k_stage (fluxes + update, fused) + k_wall (wall BC +
-// pressure BC).  k_stats runs every istat steps.
+// pressure BC).  k_stats_part + k_stats_fin run every istat steps.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -377,13 +377,16 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     const long long vol = P.vol, plane = P.plane;
     const long long colo = (long long)j * P.px + i;
 
-    auto slot = [&](int m) -> Slot {
-        const int s = m % 3;
-        return Slot{sPr + (s * 4 + 0) * NB, sPr + (s * 4 + 1) * NB, sPr + (s * 4 + 2) * NB, sPr + (s * 4 + 3) * NB};
+    // ring slots by role, rotated once per plane instead of indexed by plane:
+    // prims (u,v,w,T) for t-1, t, t+1 at offsets oM, oZ, oP; Q and (mu,p) for
+    // t, t+1 at qZ, qP and mZ, mP (offsets in doubles)
+    int oM = 0, oZ = 4 * NB, oP = 8 * NB, qZ = 0, qP = 5 * NB, mZ = 0, mP = 2 * NB;
+    auto slot = [&](int o) -> Slot {
+        return Slot{sPr + o, sPr + o + NB, sPr + o + 2 * NB, sPr + o + 3 * NB};
     };
-    auto smu = [&](int m) { return sMP + ((m & 1) * 2 + 0) * NB; };
-    auto spr = [&](int m) { return sMP + ((m & 1) * 2 + 1) * NB; };
-    auto sq = [&](int m, int v) { return sQ + ((m & 1) * 5 + v) * NB; };
+    auto smu = [&](int o) { return sMP + o; };
+    auto spr = [&](int o) { return sMP + o + NB; };
+    auto sq = [&](int o, int v) { return sQ + o + v * NB; };
 
     // box points this thread loads: the same columns for every plane
     // lp: box index | 0x10000 if the point is in R1 (tile plus a 1-point cross
@@ -410,9 +413,9 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     // of its image (whose wall values may differ from the duplicate's own
     // under a non-periodic wall BC).  hD on a wall plane reads the wall's own
     // values from memory instead (hflux_wall).
-    auto load_plane = [&](int m) {
-        const Slot s = slot(m);
-        double *MU = smu(m), *PR = spr(m);
+    auto load_plane = [&](int m, int po, int qo, int mo) {
+        const Slot s = slot(po);
+        double *MU = smu(mo), *PR = spr(mo);
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
 #pragma unroll
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 q[v] = __ldg(P.qin + v * vol + off);
-                sq(m, v)[p] = q[v];
+                sq(qo, v)[p] = q[v];
             }
             double u, vv, w, T, mu, pr;
             if (wall) {
@@ -464,11 +467,11 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     };
 
     // hD at the own column of interior plane m (in ring); dz from (m-1, m+1) values
-    auto hflux = [&](int m, double um, double vm, double wm, double Tm, double up, double vp, double wp_,
-                     double Tp, double h[4]) {
-        const Slot s = slot(m);
+    auto hflux = [&](int m, int po, int mo, double um, double vm, double wm, double Tm, double up, double vp,
+                     double wp_, double Tp, double h[4]) {
+        const Slot s = slot(po);
         const double sc = P.czh[m];
-        visc_fz<BX>(P, s, smu(m)[bc], spr(m)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
+        visc_fz<BX>(P, s, smu(mo)[bc], spr(mo)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
                     (Tp - Tm) * sc, h);
     };
     // hD at the own column of wall plane m, from the wall's own values in
@@ -492,11 +495,11 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     // ---------------- prologue: planes kb-1 and kb, hD(kb-1), hD(kb)
     double qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
     double wm2 = 0.0;
-    load_plane(kb - 1);
-    load_plane(kb);
+    load_plane(kb - 1, oM, qP, mP);
+    load_plane(kb, oZ, qZ, mZ);
     __syncthreads();
     {
-        const Slot sA = slot(kb - 1), sB = slot(kb);
+        const Slot sA = slot(oM), sB = slot(oZ);
         if (col_ok) {
             // hD(kb-1)
             if (kb - 1 == 1) {
@@ -504,13 +507,13 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             } else {
                 double q[5], u, v, w, T;
                 center(kb - 2, q, u, v, w, T);
-                hflux(kb - 1, u, v, w, T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                hflux(kb - 1, oM, mP, u, v, w, T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
             }
             // hD(kb)
             {
                 double q[5], u, v, w, T;
                 center(kb + 1, q, u, v, w, T);
-                hflux(kb, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], u, v, w, T, h0);
+                hflux(kb, oZ, mZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], u, v, w, T, h0);
             }
             if (kb - 2 >= 1) {
                 double u, v, w, T;
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 for (int c = 0; c < 4; c++) P.hwt[c * plane + colo] = h[c];
             }
 #pragma unroll
-            for (int c = 0; c < 5; c++) qm1[c] = sq(kb - 1, c)[bc];
+            for (int c = 0; c < 5; c++) qm1[c] = sq(qP, c)[bc];
         } else {
 #pragma unroll
             for (int c = 0; c < 5; c++) qm1[c] = 0.0;
@@ -536,21 +539,21 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 
     for (int t = kb; t <= ke; t++) {
         // ---------- A: plane t+1 into the ring; own column of t+2
-        load_plane(t + 1);
+        load_plane(t + 1, oP, qP, mP);
         double qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
         if (col_ok && t + 2 <= n3) center(t + 2, qp2, up2, vp2, wp2, Tp2);
         __syncthreads();
 
         // ---------- C: viscous flux vectors
-        const Slot s0 = slot(t), sm = slot(t - 1), sp = slot(t + 1);
+        const Slot s0 = slot(oZ), sm = slot(oM), sp = slot(oP);
         double hp1[4] = {0, 0, 0, 0};
         // RK base state of the own point, fetched early (stages that use it)
         {
             const double czt = P.czh[t];
-            const double *MU = smu(t), *PR = spr(t);
+            const double *MU = smu(mZ), *PR = spr(mZ);
             if (col_ok) {
                 if (t + 1 != n3)
-                    hflux(t + 1, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+                    hflux(t + 1, oP, mP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 double f[4], g[4];
                 visc_fxy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f, g);
 #pragma unroll
@@ -586,11 +589,11 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         // ---------- E: fluxes, source, RK update
         double q0[5];
 #pragma unroll
-        for (int c = 0; c < 5; c++) q0[c] = sq(t, c)[bc];
+        for (int c = 0; c < 5; c++) q0[c] = sq(qZ, c)[bc];
         const double wm1 = sm.W[bc];
         if (out_ok) {
             double R[5];
-            const double mu0 = smu(t)[bc];
+            const double mu0 = smu(mZ)[bc];
             // x
             {
                 const double *U = s0.U;
@@ -600,7 +603,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 double F1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const double *Q = sq(t, c);
+                    const double *Q = sq(qZ, c);
                     F1[c] = wsum(w, Q[bc - 2], Q[bc - 1], Q[bc], Q[bc + 1], Q[bc + 2]);
                 }
                 R[0] = F1[0];  // F2 of continuity is zero
@@ -620,7 +623,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 double G1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const double *Q = sq(t, c);
+                    const double *Q = sq(qZ, c);
                     G1[c] = wsum(w, Q[bc - 2 * BX], Q[bc - BX], Q[bc], Q[bc + BX], Q[bc + 2 * BX]);
                 }
                 R[0] = R[0] + G1[0];
@@ -643,11 +646,11 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                     inv_weights(wm2, wm1, w0, wp1, wp2, qk, P.cz8[t], P.cz12[t], w);
                 }
                 const double czt = P.czh[t];
-                R[0] = R[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(t + 1, 0)[bc], qp2[0]);
+                R[0] = R[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(qP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const double H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(t + 1, c)[bc], qp2[c]);
+                    const double H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(qP, c)[bc], qp2[c]);
                     const double hp = top ? P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
                     const double H2 = (hp - hm1[c - 1]) * czt;
                     R[c] = (R[c] + H1) + H2;
@@ -716,6 +719,12 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         for (int c = 0; c < 4; c++) {
             hm1[c] = h0[c];
             h0[c] = hp1[c];
+        }
+        {
+            const int o = oM;
+            oM = oZ; oZ = oP; oP = o;
+            int x = qZ; qZ = qP; qP = x;
+            x = mZ; mZ = mP; mP = x;
         }
         __syncthreads();
     }
@@ -812,7 +821,7 @@ __global__ void k_wall(const KParams P)
             const double E = q4 / q0;
             T = E - P.ggMh * ((u * u + v * v) + w * w);
             p = (r * T) / P.gM2;
-            mu = pow(T, 0.7);
+            mu = pow07(T);
         };
         // wall-point terms c0*mu_w*u_w of the neighbours (zero for a no-slip wall)
         double t_ip = 0.0, t_im = 0.0, t_jp = 0.0, t_jm = 0.0;
@@ -897,8 +906,7 @@ __device__ __forceinline__ void ref_var(const KParams &P, const double *q, int i
 }
 
 // Plane moments (avgSpatial, main_v1.9.f90:995-1025) and wall shear
-// (calcTauWall, main_v1.9.f90:930-977).  Blocks 0..n3-1: plane k=b+1;
-// block n3: tauL; block n3+1: tauU.  Fixed-order reductions: deterministic.
+// (calcTauWall, main_v1.9.f90:930-977), in two passes.
 constexpr int kStatThreads = 256;
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -908,21 +916,28 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-__global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const double *q, int do_moments,
-                                                        int do_tau)
+// Pass 1: block (pb, sub) sums the points sub, sub+S, ... (in units of
+// kStatThreads) of plane pb (pb < n3: the 23 moment sums of plane k = pb+1;
+// pb = n3, n3+1: the wall-shear sum of the bottom, top wall) into
+// part[(pb*S + sub)*23 + c].  Pass 2 adds the S partial sums in a fixed
+// order: the result is deterministic.
+__global__ void __launch_bounds__(kStatThreads) k_stats_part(const KParams P, const double *q, int do_moments,
+                                                             int do_tau, int S, double *part)
 {
     __shared__ double red[kStatThreads / 32][23];
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
-    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pb = blockIdx.x / S, sub = blockIdx.x - pb * S;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (frozen(P.status, P.step + 1)) return;
-    if (b < n3) {
+    double *out = part + ((size_t)pb * S + sub) * 23;
+    if (pb < n3) {
         if (!do_moments) return;
-        const int k = b + 1;
+        const int k = pb + 1;
         double acc[23];
 #pragma unroll
         for (int c = 0; c < 23; c++) acc[c] = 0.0;
         const int np = n1 * n2;
-        for (int p = tid; p < np; p += kStatThreads) {
+        for (int p = sub * kStatThreads + tid; p < np; p += S * kStatThreads) {
             const int jj = p / n1, ii = p - jj * n1;
             double x[7];
             ref_var(P, q, ii + 1, jj + 1, k, x);
@@ -950,25 +965,18 @@ __global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const d
         if (tid < 23) {
             double s = 0.0;
             for (int w = 0; w < kStatThreads / 32; w++) s += red[w][tid];
-            const double nxy = (double)(n1 * n2);
-            double *out;
-            if (tid < 7) out = P.stat + (size_t)tid * n3;
-            else if (tid < 14) out = P.stat + (size_t)7 * n3 + (size_t)(tid - 7) * n3;
-            else out = P.stat + (size_t)14 * n3 + (size_t)(tid - 14) * n3;
-            const double val = s / nxy;
-            out[k - 1] = val;
-            if (P.acc_on) P.tacc[(out - P.stat) + (k - 1)] += val;
+            out[tid] = s;
         }
         return;
     }
     if (!do_tau) return;
-    const int wall = b - n3;
+    const int wall = pb - n3;
     const double *W = P.wp + (size_t)wall * 8 * P.plane;
     const double *c = wall == 0 ? P.f1 : P.b1;
     const int k2 = wall == 0 ? 2 : n3 - 1, k3 = wall == 0 ? 3 : n3 - 2;
     double acc = 0.0;
     const int ni = n1 - 2, np = (n1 - 2) * (n2 - 2);
-    for (int p = tid; p < np; p += kStatThreads) {
+    for (int p = sub * kStatThreads + tid; p < np; p += S * kStatThreads) {
         const int jj = 2 + p / ni, ii = 2 + p % ni;
         const long long o = (long long)jj * P.px + ii;
         const double mu = W[7 * P.plane + o];
@@ -985,10 +993,40 @@ __global__ void __launch_bounds__(kStatThreads) k_stats(const KParams P, const d
     if (tid == 0) {
         double t = 0.0;
         for (int w = 0; w < kStatThreads / 32; w++) t += red[w][0];
-        const double val = t / (double)np;
-        P.stat[(size_t)23 * n3 + wall] = val;
-        if (P.acc_on) P.tacc[(size_t)23 * n3 + wall] += val;
+        out[0] = t;
     }
+}
+
+// Pass 2: one warp per plane / wall adds the S partial sums in order and
+// writes stat1Spc, stat2Spc, corrSpc (divided by nP1*nP2) and tauL, tauU
+// (divided by (nP1-2)*(nP2-2)); with time averaging on, also adds them into tacc.
+__global__ void k_stats_fin(const KParams P, int do_moments, int do_tau, int S, const double *part)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const int pb = blockIdx.x, c = threadIdx.x;
+    if (frozen(P.status, P.step + 1)) return;
+    const double *in = part + (size_t)pb * S * 23;
+    if (pb < n3) {
+        if (!do_moments || c >= 23) return;
+        double s = 0.0;
+        for (int u = 0; u < S; u++) s += in[(size_t)u * 23 + c];
+        const double nxy = (double)(n1 * n2);
+        double *out;
+        if (c < 7) out = P.stat + (size_t)c * n3;
+        else if (c < 14) out = P.stat + (size_t)7 * n3 + (size_t)(c - 7) * n3;
+        else out = P.stat + (size_t)14 * n3 + (size_t)(c - 14) * n3;
+        const double val = s / nxy;
+        out[pb] = val;
+        if (P.acc_on) P.tacc[(out - P.stat) + pb] += val;
+        return;
+    }
+    if (!do_tau || c != 0) return;
+    const int wall = pb - n3;
+    double s = 0.0;
+    for (int u = 0; u < S; u++) s += in[(size_t)u * 23];
+    const double val = s / (double)((n1 - 2) * (n2 - 2));
+    P.stat[(size_t)23 * n3 + wall] = val;
+    if (P.acc_on) P.tacc[(size_t)23 * n3 + wall] += val;
 }
 
 // ---------------------------------------------------------------------------

@@ -6,6 +6,7 @@
 #include "chanrhs.h"
 #include "chan_kernels.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,7 @@ namespace {
 #endif
 constexpr int TI = CHAN_TI;
 constexpr int TJ = CHAN_TJ;
+constexpr int kMaxSplit = 16;   // statistics blocks per plane, at most
 
 std::string g_init_error;
 
@@ -42,6 +44,8 @@ struct chan_ctx {
     double *q[3] = {nullptr, nullptr, nullptr};
     double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr, *tacc = nullptr;
     double *hwt = nullptr;   // hD of the top wall plane, staged inside a stage
+    double *spart = nullptr; // statistics partial sums [(nP3+2)*nsplit][23]
+    int nsplit = 1;          // blocks per plane in the statistics pass
     unsigned char *wmask[2] = {nullptr, nullptr};  // wall-BC plug-in arrays (allocated on first use)
     double *wuv[2] = {nullptr, nullptr}, *wx1[2] = {nullptr, nullptr};
     long long tavg_samples = 0;  // statistics steps summed into tacc since chan_time_avg_start
@@ -205,7 +209,10 @@ int launch_stats(chan_ctx *c, long long step, int moments, int tau)
 {
     c->kp.step = step;
     ProfScope ps(c, 2);
-    chan::k_stats<<<c->n3 + 2, chan::kStatThreads, 0, c->stream>>>(c->kp, c->q[c->cur], moments, tau);
+    chan::k_stats_part<<<(c->n3 + 2) * c->nsplit, chan::kStatThreads, 0, c->stream>>>(c->kp, c->q[c->cur], moments,
+                                                                                     tau, c->nsplit, c->spart);
+    CK(c, cudaGetLastError());
+    chan::k_stats_fin<<<c->n3 + 2, 32, 0, c->stream>>>(c->kp, moments, tau, c->nsplit, c->spart);
     CK(c, cudaGetLastError());
     return CHAN_OK;
 }
@@ -325,47 +332,65 @@ double *noalloc_scratch(int dev)
     return g_noalloc_addr[dev];
 }
 
-// plane moments of a staged slab of var planes k0..k0+nk-1; same per-plane
-// reduction order as k_stats
+// blocks per plane of the statistics pass: about 8 blocks per SM, at least
+// 4 point strides per block, at most kMaxSplit
+int stats_split(int sms, int n1, int n2, int n3)
+{
+    const long long np = (long long)n1 * n2;
+    int ns = (int)((8LL * sms + (n3 + 2) - 1) / (n3 + 2));
+    const int cap = (int)std::max<long long>(1, np / (4LL * chan::kStatThreads));
+    ns = std::min(std::min(ns, cap), kMaxSplit);
+    return std::max(ns, 1);
+}
+
+// plane moments of a staged slab of var planes k0..k0+nk-1, in the reduction
+// order of k_stats_part + k_stats_fin with S blocks per plane (so both paths
+// give the same bits): S partial sums in turn, then their ordered sum
 __global__ void __launch_bounds__(chan::kStatThreads) k_moments_slab(const double *slab, int n1, int n2, int nk,
-                                                                     int k0, int n3, double *res)
+                                                                     int k0, int n3, int S, double *res)
 {
     __shared__ double red[chan::kStatThreads / 32][23];
+    __shared__ double tot[23];
     const int kk = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long pl = (long long)n1 * n2;
-    double acc[23];
+    if (tid < 23) tot[tid] = 0.0;
+    for (int sub = 0; sub < S; sub++) {
+        double acc[23];
 #pragma unroll
-    for (int c = 0; c < 23; c++) acc[c] = 0.0;
-    for (long long p = tid; p < pl; p += chan::kStatThreads) {
-        double x[7];
+        for (int c = 0; c < 23; c++) acc[c] = 0.0;
+        for (long long p = (long long)sub * chan::kStatThreads + tid; p < pl; p += (long long)S * chan::kStatThreads) {
+            double x[7];
 #pragma unroll
-        for (int m = 0; m < 7; m++) x[m] = slab[((long long)m * nk + kk) * pl + p];
+            for (int m = 0; m < 7; m++) x[m] = slab[((long long)m * nk + kk) * pl + p];
 #pragma unroll
-        for (int m = 0; m < 7; m++) {
-            acc[m] += x[m];
-            acc[7 + m] += x[m] * x[m];
+            for (int m = 0; m < 7; m++) {
+                acc[m] += x[m];
+                acc[7 + m] += x[m] * x[m];
+            }
+            acc[14] += x[0] * x[3];
+            acc[15] += x[0] * x[5];
+            acc[16] += x[1] * x[2];
+            acc[17] += x[1] * x[3];
+            acc[18] += x[2] * x[3];
+            acc[19] += x[2] * x[5];
+            acc[20] += x[5] * x[3];
+            acc[21] += x[6] * x[3];
+            acc[22] += x[6] * x[5];
         }
-        acc[14] += x[0] * x[3];
-        acc[15] += x[0] * x[5];
-        acc[16] += x[1] * x[2];
-        acc[17] += x[1] * x[3];
-        acc[18] += x[2] * x[3];
-        acc[19] += x[2] * x[5];
-        acc[20] += x[5] * x[3];
-        acc[21] += x[6] * x[3];
-        acc[22] += x[6] * x[5];
-    }
 #pragma unroll
-    for (int c = 0; c < 23; c++) {
-        const double sum = chan::warp_sum(acc[c]);
-        if (lane == 0) red[warp][c] = sum;
+        for (int c = 0; c < 23; c++) {
+            const double sum = chan::warp_sum(acc[c]);
+            if (lane == 0) red[warp][c] = sum;
+        }
+        __syncthreads();
+        if (tid < 23) {
+            double sum = 0.0;
+            for (int w = 0; w < chan::kStatThreads / 32; w++) sum += red[w][tid];
+            tot[tid] += sum;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    if (tid < 23) {
-        double sum = 0.0;
-        for (int w = 0; w < chan::kStatThreads / 32; w++) sum += red[w][tid];
-        res[(long long)tid * n3 + k0 + kk] = sum / (double)(n1 * n2);
-    }
+    if (tid < 23) res[(long long)tid * n3 + k0 + kk] = tot[tid] / (double)(n1 * n2);
 }
 
 }  // namespace
@@ -422,6 +447,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     if ((r = dalloc(c, &c->wp, 2 * 8 * (size_t)c->plane)) || (r = dalloc(c, &c->cs, (size_t)(n3 + 2) * 28)) ||
         (r = dalloc(c, &c->tabs, 4 * (size_t)(n3 + 2))) || (r = dalloc(c, &c->stat, 23 * (size_t)n3 + 2)) ||
         (r = dalloc(c, &c->tacc, 23 * (size_t)n3 + 2)) || (r = dalloc(c, &c->hwt, 4 * (size_t)c->plane)) ||
+        (r = dalloc(c, &c->spart, 23 * (size_t)(n3 + 2) * kMaxSplit)) ||
         (r = dalloc(c, &c->dvar, 7 * (size_t)n1 * n2 * n3))) {
         g_init_error = c->err;
         chan_free(c);
@@ -508,6 +534,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
         if (eff > best + 1e-9) { best = eff; bestc = nc; }
     }
     c->nchunks = bestc;
+    c->nsplit = stats_split(sms, n1, n2, n3);
     c->kchunk = (nz + bestc - 1) / bestc;
     k.kchunk = c->kchunk;
 
@@ -903,6 +930,9 @@ int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1
     double *scr = noalloc_scratch(device);
     if (!scr) { cudaSetDevice(prev); return CHAN_ECUDA; }
     double *res = scr, *slab = scr + head;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int S = stats_split(sms, n1, n2, n3);
     const long long kslab_ll = ((long long)CHAN_NOALLOC_MAX_DOUBLES - head) / (7 * pl);
     const int kslab = (int)(kslab_ll < n3 ? kslab_ll : n3);
     // the results must start at zero: every plane is written below, and a
@@ -914,7 +944,7 @@ int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1
             e = cudaMemcpyAsync(slab + (size_t)m * nk * pl, var + ((size_t)m * n3 + k0) * pl,
                                 (size_t)nk * pl * sizeof(double), cudaMemcpyHostToDevice, 0);
         if (e == cudaSuccess) {
-            k_moments_slab<<<nk, chan::kStatThreads, 0, 0>>>(slab, n1, n2, nk, k0, n3, res);
+            k_moments_slab<<<nk, chan::kStatThreads, 0, 0>>>(slab, n1, n2, nk, k0, n3, S, res);
             e = cudaGetLastError();
         }
     }
@@ -1100,6 +1130,7 @@ void chan_free(chan_ctx *c)
     if (c->tabs) cudaFree(c->tabs);
     if (c->tacc) cudaFree(c->tacc);
     if (c->hwt) cudaFree(c->hwt);
+    if (c->spart) cudaFree(c->spart);
     for (int w = 0; w < 2; w++) {
         if (c->wmask[w]) cudaFree(c->wmask[w]);
         if (c->wuv[w]) cudaFree(c->wuv[w]);
