@@ -43,4 +43,5 @@ CASES = {
     "ref_rk2_cosine": dict(nP=(20, 14, 19), mesh="cosine", rk=RK2, Pr=0.71),
     "rk3_tanh": dict(nP=(22, 12, 21), mesh="tanh", beta=2.2, rk=RK3, Pr=0.72),
     "ragged": dict(nP=(39, 7, 11), mesh="cosine", rk=RK2, Pr=0.71),
+    "tiny": dict(nP=(8, 6, 9), mesh="tanh", beta=2.0, rk=RK3, Pr=0.72),
 }

@@ -232,3 +232,33 @@ def test_checkpoint_restart_is_bit_exact(tmp_path):
     assert c.time_average()["samples"] == ref_avg["samples"]
     assert np.array_equal(c.time_average()["mean"], ref_avg["mean"])
     assert c.nstep == 8 and c.time == a.time
+
+
+def test_checkpoint_faults_are_codes(tmp_path):
+    """Truncated, foreign and mismatched checkpoint files are reported as codes and
+    leave the context as it was (host-side fault injection)."""
+    from compchan3dmpi_b200 import ChanError
+    p, x3, jac, inv, var = make_case(nP=(20, 14, 19), quantize=False, istat=3)
+    a = Channel(p, x3, jac, inv)
+    a.init_sol_v(var)
+    a.step(2)
+    good = tmp_path / "good.ckp"
+    a.checkpoint_write(good)
+    blob = good.read_bytes()
+    (tmp_path / "trunc.ckp").write_bytes(blob[: len(blob) // 2])
+    (tmp_path / "foreign.ckp").write_bytes(b"NOTACKPT" + blob[8:])
+    before = a.download()
+    for name, code in (("trunc.ckp", -5), ("foreign.ckp", -5), ("missing.ckp", -5)):
+        with pytest.raises(ChanError) as ei:
+            a.checkpoint_read(tmp_path / name)
+        assert ei.value.code == code, (name, ei.value)
+        assert np.array_equal(a.download(), before)
+    q2, x32, jac2, inv2, var2 = make_case(nP=(22, 14, 19), quantize=False)
+    b = Channel(q2, x32, jac2, inv2)
+    b.init_sol_v(var2)
+    with pytest.raises(ChanError) as ei:
+        b.checkpoint_read(good)
+    assert ei.value.code == -1
+    a.step(1)   # still usable
+    assert a.nstep == 3
+
