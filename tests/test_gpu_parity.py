@@ -262,3 +262,29 @@ def test_checkpoint_faults_are_codes(tmp_path):
     a.step(1)   # still usable
     assert a.nstep == 3
 
+
+
+@pytest.mark.parametrize("Pe", [(1e300, 1e300, 1e300), (0.0, 0.0, 0.0)], ids=["central", "quick"])
+def test_one_scheme_everywhere(Pe):
+    """Pe thresholds never / always exceeded: the central and the QUICK branch alone."""
+    case = make_case(nP=(20, 14, 19), Pe=Pe)
+    g, o = _pair(case)
+    for s in range(1, 4):
+        g.step(1)
+        o.step(1)
+        _assert_close(g.download(), o.download(), what=f"Pe={Pe} step {s}")
+
+
+@pytest.mark.parametrize("Pe", [(1e300, 1e300, 1e300), (0.0, 0.0, 0.0)], ids=["central", "quick"])
+def test_plane_mass_conserved_on_gpu(Pe):
+    """w = 0: each interior plane's mass over its periodic points is kept by a stage
+    when one inviscid scheme is used everywhere (telescoping face fluxes)."""
+    from chan_cases import conservation_case, plane_mass
+    p, x3, jac, inv, var = conservation_case(Pe=Pe)
+    g = Channel(p, x3, jac, inv)
+    g.init_sol_v(var)
+    m0 = plane_mass(var)
+    g.stage(1)
+    m1 = plane_mass(g.download())
+    rel = np.abs(m1[1:-1] - m0[1:-1]) / m0[1:-1]
+    assert rel.max() <= 1e-13, rel.max()

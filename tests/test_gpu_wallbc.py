@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from chan_cases import CASES, make_case, rel_err, worst
-from compchan3dmpi_b200 import Channel, ChanError
+from compchan3dmpi_b200 import Channel, ChanError, RK3
 from compchan3dmpi_b200 import wallbc as W
 from oracle import oracle as O
 
@@ -92,3 +92,39 @@ def test_wall_bc_errors():
         g.set_wall_bc(0, W.isothermal(-1.0))
     with pytest.raises(ChanError):
         g.set_wall_bc(0, W.WallBC(velocity=7))
+
+
+@pytest.mark.parametrize("name", ["st4", "gst2", "s3", "rd1"])
+def test_variant_40_steps_with_forcing(name):
+    """Longer runs with the lagged forcing refreshed every 5 steps: no drift."""
+    case = make_case(nP=(24, 16, 21), mesh="tanh", beta=2.0, rk=RK3, Pr=0.72, istat=5, quantize=False)
+    bottom, top = W.reference_variant(name, case[0])
+    g, o = _pair(case, bottom, top)
+    for blk in range(4):
+        g.step(10)
+        o.step(10)
+        gv, ov = g.download(), o.download()
+        e = rel_err(gv, ov)
+        assert e.max() <= TOL, f"{name} step {10 * (blk + 1)}: {e} worst at {worst(gv, ov)}"
+
+
+def test_checkpoint_restart_with_wall_bc(tmp_path):
+    """The checkpoint holds the state, not the wall-BC setting: restore, set the BC
+    again, and the run continues bit for bit."""
+    p, x3, jac, inv, var = make_case(nP=(20, 14, 19), quantize=False, istat=3)
+    bottom, top = W.reference_variant("gst5", p)
+    a = Channel(p, x3, jac, inv)
+    a.init_sol_v(var)
+    a.set_wall_bc(0, bottom)
+    a.step(8)
+    ref = a.download()
+    b = Channel(p, x3, jac, inv)
+    b.init_sol_v(var)
+    b.set_wall_bc(0, bottom)
+    b.step(4)
+    b.checkpoint_write(tmp_path / "w.ckp")
+    c = Channel(p, x3, jac, inv)
+    c.set_wall_bc(0, bottom)
+    c.checkpoint_read(tmp_path / "w.ckp")
+    c.step(4)
+    assert np.array_equal(c.download(), ref)
