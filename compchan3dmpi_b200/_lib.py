@@ -90,6 +90,7 @@ SIGNATURES = [
     ("chan_fluctuation_q", ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D, _D, _D]),
     ("chan_q_criterion", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32), _D, _D, _D, _D, _D, _D, _D,
                                         ctypes.c_int32]),
+    ("chan_debug_canaries", ctypes.c_int, [ctypes.c_void_p, _I64]),
     ("chan_checkpoint_write", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_checkpoint_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("chan_deck_read", ctypes.c_int, [ctypes.c_char_p, _I32, _D, _D, _D, _D, _D, _I64, ctypes.c_int32]),

@@ -281,6 +281,12 @@ class Channel:
     def stream_handle(self) -> int:
         return int(self.L.chan_stream(self._h) or 0)
 
+    def debug_canaries(self) -> int:
+        """Guard words around the state buffers that changed (0: no stray writes)."""
+        n = ctypes.c_int64()
+        self._check(self.L.chan_debug_canaries(self._h, ctypes.byref(n)))
+        return n.value
+
     def device_bytes(self) -> int:
         return int(self.L.chan_device_bytes(self._h))
 

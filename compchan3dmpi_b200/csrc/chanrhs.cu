@@ -68,6 +68,11 @@ struct chan_ctx {
     std::vector<cudaEvent_t> ev_pool;
     size_t dev_bytes = 0;
     std::vector<double> hx3;      // x3 given to chan_init
+    struct Guarded {
+        double *base;
+        size_t n;
+    };
+    std::vector<Guarded> guarded;  // guard-zoned state buffers (dalloc)
     // diagnostics series (allocated by chan_diag_enable)
     int diag_every = 0, diag_cap = 0, diag_reclen = 0;
     long long diag_count = 0;     // records written since the last chan_diag_read
@@ -285,14 +290,29 @@ int read_status(chan_ctx *c, int32_t *ijk)
     return CHAN_OK;
 }
 
+// Every state buffer sits between two guard zones of kGuard words holding
+// kCanary (a NaN bit pattern no kernel writes).  chan_debug_canaries reads
+// them back: any change means a kernel wrote outside its buffer.
+constexpr size_t kGuard = 64;   // 512 bytes: the payload keeps 256-byte alignment
+constexpr unsigned long long kCanary = 0x7ff4deadbeef0001ULL;
+
 int dalloc(chan_ctx *c, double **p, size_t n)
 {
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(double));
+    double *base = nullptr;
+    cudaError_t e = cudaMalloc((void **)&base, (n + 2 * kGuard) * sizeof(double));
     if (e != cudaSuccess) {
         fail(c, "cudaMalloc", e);
         return CHAN_ENOMEM;
     }
-    c->dev_bytes += n * sizeof(double);
+    c->guarded.push_back({base, n});
+    c->dev_bytes += (n + 2 * kGuard) * sizeof(double);
+    *p = base + kGuard;
+    std::vector<unsigned long long> pat(kGuard, kCanary);
+    e = cudaMemcpyAsync(base, pat.data(), kGuard * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + kGuard + n, pat.data(), kGuard * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);   // pat is a host temporary
+    if (e != cudaSuccess) return fail(c, "guard fill", e);
     e = cudaMemsetAsync(*p, 0, n * sizeof(double), c->stream);
     if (e != cudaSuccess) return fail(c, "cudaMemsetAsync", e);
     return CHAN_OK;
@@ -1117,6 +1137,24 @@ int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const 
     return rc;
 }
 
+int chan_debug_canaries(chan_ctx *c, int64_t *corrupted)
+{
+    if (!c || !corrupted) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    CK(c, cudaStreamSynchronize(c->stream));
+    int64_t bad = 0;
+    std::vector<unsigned long long> h(kGuard);
+    for (const auto &g : c->guarded) {
+        for (int side = 0; side < 2; side++) {
+            const double *src = side == 0 ? g.base : g.base + kGuard + g.n;
+            CK(c, cudaMemcpy(h.data(), src, kGuard * sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t w = 0; w < kGuard; w++) bad += h[w] != kCanary;
+        }
+    }
+    *corrupted = bad;
+    return CHAN_OK;
+}
+
 void chan_free(chan_ctx *c)
 {
     if (!c) return;
@@ -1124,20 +1162,13 @@ void chan_free(chan_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &pp : c->prof_pairs) { cudaEventDestroy(pp.a); cudaEventDestroy(pp.b); }
     for (auto e : c->ev_pool) cudaEventDestroy(e);
-    for (int b = 0; b < 3; b++) if (c->q[b]) cudaFree(c->q[b]);
-    if (c->wp) cudaFree(c->wp);
-    if (c->cs) cudaFree(c->cs);
-    if (c->tabs) cudaFree(c->tabs);
-    if (c->tacc) cudaFree(c->tacc);
-    if (c->hwt) cudaFree(c->hwt);
-    if (c->spart) cudaFree(c->spart);
+    for (auto &g : c->guarded) cudaFree(g.base);
     for (int w = 0; w < 2; w++) {
         if (c->wmask[w]) cudaFree(c->wmask[w]);
         if (c->wuv[w]) cudaFree(c->wuv[w]);
         if (c->wx1[w]) cudaFree(c->wx1[w]);
     }
-    if (c->stat) cudaFree(c->stat);
-    if (c->dvar) cudaFree(c->dvar);
+
     if (c->diag_rec) cudaFree(c->diag_rec);
     if (c->diag_part) cudaFree(c->diag_part);
     if (c->diag_x3) cudaFree(c->diag_x3);

@@ -27,20 +27,27 @@ class DeckError(ValueError):
 
 
 # ------------------------------------------------------------------ E22.15
-def fmt_e22_15(x: float) -> str:
-    """Fortran E22.15 output: 0.ddddddddddddddd E+xx, right-justified to 22."""
+def fmt_e(x: float, w: int, d: int) -> str:
+    """Fortran Ew.d output: [-]0.<d digits>E+xx, right-justified in w columns
+    (3-digit exponents drop the letter: 0.123+100)."""
     if x != x or math.isinf(x):
-        return ("NaN" if x != x else ("-Infinity" if x < 0 else "Infinity")).rjust(22)
+        return ("NaN" if x != x else ("-Infinity" if x < 0 else "Infinity")).rjust(w)
     neg = math.copysign(1.0, x) < 0 and x != 0.0
     if x == 0.0:
-        body = "0.000000000000000E+00"
+        body = "0." + "0" * d + "E+00"
     else:
-        s = f"{abs(x):.14E}"
+        s = f"{abs(x):.{d - 1}E}"
         mant, ex = s.split("E")
         digits = mant.replace(".", "")
         e = int(ex) + 1
         body = f"0.{digits}E{e:+03d}" if abs(e) <= 99 else f"0.{digits}{e:+04d}"
-    return (("-" if neg else "") + body).rjust(22)
+    out = ("-" if neg else "") + body
+    return out.rjust(w) if len(out) <= w else "*" * w
+
+
+def fmt_e22_15(x: float) -> str:
+    """Fortran E22.15 output: 0.ddddddddddddddd E+xx, right-justified to 22."""
+    return fmt_e(x, 22, 15)
 
 
 def parse_fortran_real(s: str) -> float:

@@ -307,6 +307,13 @@ int chan_fluctuation_q(chan_ctx *c, const double *mean, const double *x1, const 
 int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const double *w, const double *x1,
                      const double *x2, const double *x3, double *qcrit, int32_t device);
 
+/* Out-of-bounds write detector.  Every state buffer of a context sits
+ * between two 512-byte guard zones filled with a NaN bit pattern that no
+ * kernel writes; this waits for queued work and counts the guard words that
+ * changed (0 when every write stayed inside its buffer).  A substitute for a
+ * memory checker in tests; the reference has no counterpart. */
+int chan_debug_canaries(chan_ctx *c, int64_t *corrupted);
+
 /* Free device memory and the context.  NULL is allowed. */
 void chan_free(chan_ctx *c);
 

@@ -288,3 +288,25 @@ def test_plane_mass_conserved_on_gpu(Pe):
     m1 = plane_mass(g.download())
     rel = np.abs(m1[1:-1] - m0[1:-1]) / m0[1:-1]
     assert rel.max() <= 1e-13, rel.max()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_no_write_outside_buffers(name):
+    """Guard zones around every state buffer stay intact through stages, steps,
+    statistics, diagnostics, wall-BC plug-ins, downloads and checkpoints."""
+    from compchan3dmpi_b200 import wallbc as W
+    p, x3, jac, inv, var = make_case(**CASES[name])
+    g = Channel(p, x3, jac, inv)
+    g.init_sol_v(var)
+    assert g.debug_canaries() == 0
+    g.diag_enable((3, 5, 70), every=2)
+    g.time_avg_start()
+    g.stage(1)
+    g.step(3)
+    g.set_wall_bc(0, W.reference_variant("gst3", p)[0])
+    g.set_wall_bc(1, W.reference_variant("rd1", p)[0])
+    g.step(4)
+    g.calc_tau_wall(); g.avg_spatial(); g.stats(); g.diag_read(); g.time_average()
+    g.fluctuation_q(np.ones((7, p.nP[2])))
+    g.download()
+    assert g.debug_canaries() == 0

@@ -184,3 +184,17 @@ def test_native_deck_reports_bad_records(tmp_path):
         read_3d_dat_native(tmp_path / "bad.dat", p.nP)
     with pytest.raises(DeckError, match="cannot open"):
         read_3d_dat_native(tmp_path / "missing.dat", p.nP)
+
+
+def test_driver_event_cadence_and_debug_format(tmp_path):
+    from compchan3dmpi_b200.run import _next_event, write_debug_dump
+    assert _next_event(0, 50, 7) == 7
+    assert _next_event(7, 50, 7) == 10
+    assert _next_event(995, 5000, 0) == 1000
+    assert _next_event(48, 50, 10) == 50
+    var = np.zeros((7, 2, 2, 2)); var[0] = 1.5; var[5] = -2.5e-3
+    write_debug_dump(tmp_path / "d.dat", var, [0.0, 1.0], [0.0, 0.5], [0.0, 2.0], 0.25, 7)
+    lines = (tmp_path / "d.dat").read_text().splitlines()
+    assert lines[0] == 'TITLE ="        0.2500000000        7"'
+    assert lines[5] == "  0.0000  0.0000  0.0000  0.15000E+01  0.00000E+00  0.00000E+00  0.00000E+00" \
+                       "  0.00000E+00 -0.25000E-02  0.00000E+00"
