@@ -47,8 +47,9 @@ def workload(nP=GRID):
 
 def config_dict(p, n_gpus):
     n1, n2, n3 = p.nP
+    kind = "mixed FP32/FP64 DNS" if getattr(p, "mixed", False) else "plain FP64 DNS"
     return {
-        "workload": f"plain FP64 DNS {n1}x{n3}x{n2} (x*wall-normal*spanwise), SSP-RK3 CFL {CFL}, "
+        "workload": f"{kind} {n1}x{n3}x{n2} (x*wall-normal*spanwise), SSP-RK3 CFL {CFL}, "
                     f"tanh beta {BETA}",
         "nP": list(p.nP),
         "points": n1 * n2 * n3,
@@ -166,6 +167,30 @@ def cpu_baseline(nP=GRID, budget_s=20.0, threads=None):
                       f"(no Fortran compiler on this image)"}
 
 
+def mixed_error(p, x3, jac, inv, var, steps=200, every=50):
+    """Relative L2 error per variable of the mixed-precision path against the
+    plain FP64 path (which matches the oracle to 1e-12) from the same start."""
+    import torch
+    from compchan3dmpi_b200 import Channel
+    a = Channel(p, x3, jac, inv)
+    b = Channel(p.with_(mixed=False), x3, jac, inv)
+    a.init_sol_v(var)
+    b.init_sol_v(var)
+    out = []
+    for s in range(every, steps + 1, every):
+        a.step(every)
+        b.step(every)
+        ga = torch.from_numpy(a.download()).cuda()
+        gb = torch.from_numpy(b.download()).cuda()
+        e = [float(torch.linalg.vector_norm(ga[m] - gb[m]) / torch.linalg.vector_norm(gb[m])) for m in range(7)]
+        out.append({"step": s, "rel_l2": e})
+        del ga, gb
+    a.close()
+    b.close()
+    return {"reference": "plain FP64 path, same start", "per_step": out,
+            "max_rel_l2": max(max(r["rel_l2"]) for r in out)}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (the oracle port) on the
     host cores, same metric/config; rank 0 only."""
@@ -223,7 +248,7 @@ def run_ours(args):
     dev = ranks.local_rank
     torch.cuda.set_device(dev)
     p, x3, jac, inv, var = workload(tuple(args.grid))
-    p = p.with_(device=dev)
+    p = p.with_(device=dev, mixed=bool(args.mixed))
     n_int = p.n_interior
     K, W = args.steps, args.warmup
 
@@ -296,16 +321,21 @@ def run_ours(args):
         stages = p.stages
         value = ranks.world * n_int * stages * K / (ms_max / 1e3)
         e2e_val = ranks.world * n_int * stages * K / (e2e_ms / 1e3)
-        bpp = (80 + 120 * (stages - 1)) / stages   # algorithmic bytes per updated point per stage launch
+        if p.mixed:
+            # stage 1 reads the double state and writes float; middle stages read float and
+            # the double base and write float; the last writes the double state
+            bpp = ((40 + 20) + (20 + 40 + 20) * (stages - 2) + (20 + 40 + 40)) / stages
+        else:
+            bpp = (80 + 120 * (stages - 1)) / stages   # algorithmic bytes per updated point per stage launch
         achieved = n_int * bpp / (stage_ms_max / 1e3) / 1e9
         peak, peak_kind = hbm_peak()
-        traffic = measured_traffic(p, n_int)
+        traffic = None if p.mixed else measured_traffic(p, n_int)
         # stage + wall-BC kernels per stage, plus the two statistics passes on their cadence
         launches = K * 2 * stages + 2 * sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded laminar Poiseuille +-10%)",
+            "dtype": "f32+f64" if p.mixed else "f64", "data": "synthetic (seeded laminar Poiseuille +-10%)",
             "config": config_dict(p, ranks.world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -319,6 +349,8 @@ def run_ours(args):
             "clocks": ck,
             "status_ok": status_ok,
         }
+        if p.mixed:
+            line["mixed_error"] = mixed_error(p, x3, jac, inv, var)
         if ranks.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(tuple(args.grid), budget_s=args.cpu_budget)
         print(json.dumps(line), flush=True)
@@ -335,6 +367,8 @@ def main():
     ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--mixed", action="store_true",
+                    help="mixed precision: float stage storage and fluxes, double accumulation")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -16,6 +16,7 @@ LIBNAME = "libchanrhs.so"
 
 CHAN_OK, CHAN_BLOWUP, CHAN_NONFINITE = 0, 1, 2
 CHAN_EINVAL, CHAN_ENOMEM, CHAN_ECUDA, CHAN_ESTATE, CHAN_EIO = -1, -2, -3, -4, -5
+CHAN_MIXED = 1
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I32 = ctypes.POINTER(ctypes.c_int32)

@@ -47,7 +47,7 @@ def to_c_params(p: ChanParams) -> _lib.ChanParamsC:
     c.rk_scheme = int(p.rk_scheme)
     c.forcing = int(p.forcing)
     c.device = int(p.device)
-    c.flags = 0
+    c.flags = _lib.CHAN_MIXED if getattr(p, "mixed", False) else 0
     c.Re = float(p.Re); c.Mac = float(p.Mac); c.dt = float(p.dt); c.Pr = float(p.Pr); c.gama = float(p.gama)
     c.Pe[:] = [float(x) for x in p.Pe]
     c.Lx = float(p.Lx); c.Ly = float(p.Ly)

@@ -20,6 +20,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 
 namespace chan {
 
@@ -45,13 +46,27 @@ struct WallBC {
     const double *x1;           // [nP1] x coordinates for the wave
 };
 
+// Flux arithmetic is templated on its real type R: double for the plain FP64
+// path, float for the mixed-precision path (FP32 fluxes and stage storage,
+// FP64 primitive recovery, RK accumulation and reductions).  FluxC holds the
+// constants the flux formulas use, in R.
+template <typename R>
+struct FluxC {
+    R invRe, ggM, two3rd, kq, inv_gM2;
+    R hdx, hdy, sx8, sx12, sy8, sy12;
+    R pex, pey, PexVal, PeyVal, pez_val;
+};
+
 struct KParams {
     // geometry
     int n1, n2, n3, px, NJ, kchunk;
     long long plane, vol;
-    // state
-    const double *qin, *qbase;
-    double *qout;
+    // state: stage input and output in the stage's storage type (double, or
+    // float for the intermediate stages of the mixed-precision path); the RK
+    // base state is always double
+    const void *qin;
+    const double *qbase;
+    void *qout;
     double *wp;
     const double *cs;
     // per-k tables [nP3+2]
@@ -59,6 +74,7 @@ struct KParams {
     const double *cz8;    // invdXi*invJac(k)/8
     const double *cz12;   // invdXi*invJac(k)/12
     const double *pez;    // Re*dXi*jac(k)
+    const float *tabf;    // the same four tables in float, [4][nP3+2] (mixed precision)
     // forcing / stats
     double *stat;         // stat1[7*n3] | stat2[7*n3] | corr[9*n3] | tau[2]
     double *tacc;         // running sums of the same 23*n3+2 numbers over statistics steps
@@ -71,6 +87,8 @@ struct KParams {
     double PexVal, PeyVal;
     double inv_dz1, inv_dzN;
     double Twb, Twt, muwb, muwt;
+    FluxC<double> cd;     // flux constants in double (plain FP64 path)
+    FluxC<float> cf;      // and in float (mixed-precision path)
     double f1[3], f2[3], b1[3], b2[3];  // wall one-sided coefficients
     // RK stage
     double rk_a, rk_b, rk_cdt;
@@ -114,17 +132,17 @@ __device__ __forceinline__ void flag_nonfinite(DevStatus *st, int i, int j, int 
 //  central : (-u2 Q2 + 8 u1 Q1 - 8 u-1 Q-1 + u-2 Q-2) /(12 d)   main_v1.9.f90:364-368
 //  QUICK   : ue*Qe - uw*Qw, face values upwinded on the face velocity sign,
 //            the four sign branches of main_v1.9.f90:335-361
-__device__ __forceinline__ void inv_weights(double um2, double um1, double u0, double up1, double up2,
-                                            bool quick, double s8, double s12, double w[5])
+template <typename R>
+__device__ __forceinline__ void inv_weights(R um2, R um1, R u0, R up1, R up2, bool quick, R s8, R s12, R w[5])
 {
     if (quick) {
-        const double r1 = (u0 + up1) * 0.5;  // tmpR1, east face
-        const double r2 = (u0 + um1) * 0.5;  // tmpR2, west face
-        const bool e = r1 >= 0.0, f = r2 >= 0.0;
-        const double R1 = r1 * s8, R2 = r2 * s8;
+        const R r1 = (u0 + up1) * R(0.5);  // tmpR1, east face
+        const R r2 = (u0 + um1) * R(0.5);  // tmpR2, west face
+        const bool e = r1 >= R(0), f = r2 >= R(0);
+        const R R1 = r1 * s8, R2 = r2 * s8;
         // east face value at offsets -1,0,+1,+2 ; west face at -2,-1,0,+1
-        const double ae_m1 = e ? -1.0 : 0.0, ae_0 = e ? 6.0 : 3.0, ae_1 = e ? 3.0 : 6.0, ae_2 = e ? 0.0 : -1.0;
-        const double bw_m2 = f ? -1.0 : 0.0, bw_m1 = f ? 6.0 : 3.0, bw_0 = f ? 3.0 : 6.0, bw_1 = f ? 0.0 : -1.0;
+        const R ae_m1 = e ? R(-1) : R(0), ae_0 = e ? R(6) : R(3), ae_1 = e ? R(3) : R(6), ae_2 = e ? R(0) : R(-1);
+        const R bw_m2 = f ? R(-1) : R(0), bw_m1 = f ? R(6) : R(3), bw_0 = f ? R(3) : R(6), bw_1 = f ? R(0) : R(-1);
         w[0] = -R2 * bw_m2;
         w[1] = R1 * ae_m1 - R2 * bw_m1;
         w[2] = R1 * ae_0 - R2 * bw_0;
@@ -132,14 +150,15 @@ __device__ __forceinline__ void inv_weights(double um2, double um1, double u0, d
         w[4] = R1 * ae_2;
     } else {
         w[0] = um2 * s12;
-        w[1] = -8.0 * um1 * s12;
-        w[2] = 0.0;
-        w[3] = 8.0 * up1 * s12;
+        w[1] = R(-8) * um1 * s12;
+        w[2] = R(0);
+        w[3] = R(8) * up1 * s12;
         w[4] = -(up2 * s12);
     }
 }
 
-__device__ __forceinline__ double wsum(const double w[5], double q0, double q1, double q2, double q3, double q4)
+template <typename R>
+__device__ __forceinline__ R wsum(const R w[5], R q0, R q1, R q2, R q3, R q4)
 {
     return (((w[0] * q0 + w[1] * q1) + w[2] * q2) + w[3] * q3) + w[4] * q4;
 }
@@ -149,119 +168,119 @@ __device__ __forceinline__ double wsum(const double w[5], double q0, double q1, 
 // fD2..fD5 (fD1 = 0).  The energy component uses the identity
 //   ggM*u*p + dissF = ggM*(u*fD2 + v*fD3 + w*fD4),
 // which is the reference's dissF regrouped (same terms, different rounding).
-struct Slot {
-    const double *U, *V, *W, *T;
+template <typename R>
+struct SlotT {
+    const R *U, *V, *W, *T;
 };
 
-template <int BX>
-__device__ __forceinline__ void visc_fx(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
-                                        const double *MU, const double *PR, int b, double czt, double f[4])
+template <int BX, typename R>
+__device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
+                                        const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4])
 {
-    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
-    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
-    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
-    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
-    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
-    const double Tx = (s.T[b + 1] - s.T[b - 1]) * P.hdx;
-    const double uz = (sp.U[b] - sm.U[b]) * czt;
-    const double wz = (sp.W[b] - sm.W[b]) * czt;
-    const double mu = MU[b], pr = PR[b];
-    const double mr = mu * P.invRe;
-    const double div = (ux + vy) + wz;
-    const double f2 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * ux;
-    const double f3 = -(mr * (vx + uy));
-    const double f4 = -(mr * (wx + uz));
+    const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
+    const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
+    const R vx = (s.V[b + 1] - s.V[b - 1]) * C.hdx;
+    const R vy = (s.V[b + BX] - s.V[b - BX]) * C.hdy;
+    const R wx = (s.W[b + 1] - s.W[b - 1]) * C.hdx;
+    const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
+    const R uz = (sp.U[b] - sm.U[b]) * czt;
+    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R mu = MU[b], pr = PR[b];
+    const R mr = mu * C.invRe;
+    const R div = (ux + vy) + wz;
+    const R f2 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * ux;
+    const R f3 = -(mr * (vx + uy));
+    const R f4 = -(mr * (wx + uz));
     f[0] = f2;
     f[1] = f3;
     f[2] = f4;
-    f[3] = -((P.kq * mu) * Tx) + P.ggM * ((s.U[b] * f2 + s.V[b] * f3) + s.W[b] * f4);
+    f[3] = -((C.kq * mu) * Tx) + C.ggM * ((s.U[b] * f2 + s.V[b] * f3) + s.W[b] * f4);
 }
 
-template <int BX>
-__device__ __forceinline__ void visc_fy(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
-                                        const double *MU, const double *PR, int b, double czt, double g[4])
+template <int BX, typename R>
+__device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
+                                        const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R g[4])
 {
-    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
-    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
-    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
-    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
-    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
-    const double Ty = (s.T[b + BX] - s.T[b - BX]) * P.hdy;
-    const double vz = (sp.V[b] - sm.V[b]) * czt;
-    const double wz = (sp.W[b] - sm.W[b]) * czt;
-    const double mu = MU[b], pr = PR[b];
-    const double mr = mu * P.invRe;
-    const double div = (ux + vy) + wz;
-    const double g2 = -(mr * (vx + uy));
-    const double g3 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * vy;
-    const double g4 = -(mr * (wy + vz));
+    const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
+    const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
+    const R vx = (s.V[b + 1] - s.V[b - 1]) * C.hdx;
+    const R vy = (s.V[b + BX] - s.V[b - BX]) * C.hdy;
+    const R wy = (s.W[b + BX] - s.W[b - BX]) * C.hdy;
+    const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
+    const R vz = (sp.V[b] - sm.V[b]) * czt;
+    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R mu = MU[b], pr = PR[b];
+    const R mr = mu * C.invRe;
+    const R div = (ux + vy) + wz;
+    const R g2 = -(mr * (vx + uy));
+    const R g3 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * vy;
+    const R g4 = -(mr * (wy + vz));
     g[0] = g2;
     g[1] = g3;
     g[2] = g4;
-    g[3] = -((P.kq * mu) * Ty) + P.ggM * ((s.U[b] * g2 + s.V[b] * g3) + s.W[b] * g4);
+    g[3] = -((C.kq * mu) * Ty) + C.ggM * ((s.U[b] * g2 + s.V[b] * g3) + s.W[b] * g4);
 }
 
 // fD and gD together at one point: they share eight gradients, the shear
 // stress mu*(dv/dx+du/dy) (fD3 = gD2) and p + 2/3*mu*div.
-template <int BX>
-__device__ __forceinline__ void visc_fxy(const KParams &P, const Slot &s, const Slot &sm, const Slot &sp,
-                                         const double *MU, const double *PR, int b, double czt, double f[4],
-                                         double g[4])
+template <int BX, typename R>
+__device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
+                                         const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4], R g[4])
 {
-    const double ux = (s.U[b + 1] - s.U[b - 1]) * P.hdx;
-    const double uy = (s.U[b + BX] - s.U[b - BX]) * P.hdy;
-    const double vx = (s.V[b + 1] - s.V[b - 1]) * P.hdx;
-    const double vy = (s.V[b + BX] - s.V[b - BX]) * P.hdy;
-    const double wx = (s.W[b + 1] - s.W[b - 1]) * P.hdx;
-    const double wy = (s.W[b + BX] - s.W[b - BX]) * P.hdy;
-    const double Tx = (s.T[b + 1] - s.T[b - 1]) * P.hdx;
-    const double Ty = (s.T[b + BX] - s.T[b - BX]) * P.hdy;
-    const double uz = (sp.U[b] - sm.U[b]) * czt;
-    const double vz = (sp.V[b] - sm.V[b]) * czt;
-    const double wz = (sp.W[b] - sm.W[b]) * czt;
-    const double mu = MU[b], pr = PR[b];
-    const double u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
-    const double mr = mu * P.invRe, kqm = P.kq * mu;
-    const double div = (ux + vy) + wz;
-    const double pd = pr + (P.two3rd * mr) * div;
-    const double t12 = mr * (vx + uy);
-    const double f2 = pd - (2.0 * mr) * ux;
-    const double f4 = -(mr * (wx + uz));
-    const double g3 = pd - (2.0 * mr) * vy;
-    const double g4 = -(mr * (wy + vz));
+    const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
+    const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
+    const R vx = (s.V[b + 1] - s.V[b - 1]) * C.hdx;
+    const R vy = (s.V[b + BX] - s.V[b - BX]) * C.hdy;
+    const R wx = (s.W[b + 1] - s.W[b - 1]) * C.hdx;
+    const R wy = (s.W[b + BX] - s.W[b - BX]) * C.hdy;
+    const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
+    const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
+    const R uz = (sp.U[b] - sm.U[b]) * czt;
+    const R vz = (sp.V[b] - sm.V[b]) * czt;
+    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R mu = MU[b], pr = PR[b];
+    const R u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
+    const R mr = mu * C.invRe, kqm = C.kq * mu;
+    const R div = (ux + vy) + wz;
+    const R pd = pr + (C.two3rd * mr) * div;
+    const R t12 = mr * (vx + uy);
+    const R f2 = pd - (R(2) * mr) * ux;
+    const R f4 = -(mr * (wx + uz));
+    const R g3 = pd - (R(2) * mr) * vy;
+    const R g4 = -(mr * (wy + vz));
     f[0] = f2;
     f[1] = -t12;
     f[2] = f4;
-    f[3] = -(kqm * Tx) + P.ggM * ((u0 * f2 - v0 * t12) + w0 * f4);
+    f[3] = -(kqm * Tx) + C.ggM * ((u0 * f2 - v0 * t12) + w0 * f4);
     g[0] = -t12;
     g[1] = g3;
     g[2] = g4;
-    g[3] = -(kqm * Ty) + P.ggM * ((-(u0 * t12) + v0 * g3) + w0 * g4);
+    g[3] = -(kqm * Ty) + C.ggM * ((-(u0 * t12) + v0 * g3) + w0 * g4);
 }
 
 // hD from its in-plane derivatives, point values and z-derivatives
-__device__ __forceinline__ void visc_fz_vals(const KParams &P, double ux, double vy, double wx, double wy, double u,
-                                             double v, double w, double mu, double pr, double uz, double vz,
-                                             double wz, double Tz, double h[4])
+template <typename R>
+__device__ __forceinline__ void visc_fz_vals(const FluxC<R> &C, R ux, R vy, R wx, R wy, R u, R v, R w, R mu, R pr,
+                                             R uz, R vz, R wz, R Tz, R h[4])
 {
-    const double mr = mu * P.invRe;
-    const double div = (ux + vy) + wz;
-    const double h2 = -(mr * (wx + uz));
-    const double h3 = -(mr * (wy + vz));
-    const double h4 = (pr + (P.two3rd * mr) * div) - (2.0 * mr) * wz;
+    const R mr = mu * C.invRe;
+    const R div = (ux + vy) + wz;
+    const R h2 = -(mr * (wx + uz));
+    const R h3 = -(mr * (wy + vz));
+    const R h4 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * wz;
     h[0] = h2;
     h[1] = h3;
     h[2] = h4;
-    h[3] = -((P.kq * mu) * Tz) + P.ggM * ((u * h2 + v * h3) + w * h4);
+    h[3] = -((C.kq * mu) * Tz) + C.ggM * ((u * h2 + v * h3) + w * h4);
 }
 
 // hD at the thread's own column; z-derivatives supplied by the caller
-template <int BX>
-__device__ __forceinline__ void visc_fz(const KParams &P, const Slot &s, double mu, double pr, int b,
-                                        double uz, double vz, double wz, double Tz, double h[4])
+template <int BX, typename R>
+__device__ __forceinline__ void visc_fz(const FluxC<R> &C, const SlotT<R> &s, R mu, R pr, int b, R uz, R vz, R wz,
+                                        R Tz, R h[4])
 {
-    visc_fz_vals(P, (s.U[b + 1] - s.U[b - 1]) * P.hdx, (s.V[b + BX] - s.V[b - BX]) * P.hdy,
-                 (s.W[b + 1] - s.W[b - 1]) * P.hdx, (s.W[b + BX] - s.W[b - BX]) * P.hdy, s.U[b], s.V[b], s.W[b],
+    visc_fz_vals(C, (s.U[b + 1] - s.U[b - 1]) * C.hdx, (s.V[b + BX] - s.V[b - BX]) * C.hdy,
+                 (s.W[b + 1] - s.W[b - 1]) * C.hdx, (s.W[b + BX] - s.W[b - BX]) * C.hdy, s.U[b], s.V[b], s.W[b],
                  mu, pr, uz, vz, wz, Tz, h);
 }
 
@@ -334,31 +353,79 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
 // Each thread keeps its own column's Q and w at t-2, t-1, t+2 and hD at
 // t-1, t, t+1 in registers.  Per output plane the CTA loads one new plane,
 // so Q is read from DRAM once per stage (halo re-reads come from L2).
-template <int TI, int TJ>
+//
+// Types: QI / QO are the storage types of the stage's input and output state,
+// R the type of the shared rings and of the flux arithmetic.  The plain FP64
+// path is <double, double, double>.  The mixed-precision path stores the
+// intermediate stage states in float and evaluates the fluxes in float; the
+// primitive recovery (T from the total energy), the RK update against the
+// double base state, the forcing and the blow-up test stay in double.
+template <int TI, int TJ, typename R>
 struct StageShape {
     static constexpr int BX = TI + 4, BY = TJ + 4, NB = BX * BY, NT = TI * TJ;
     static constexpr int NFX = TJ * (TI + 2), NGY = (TJ + 2) * TI;
-    static constexpr int doubles = 12 * NB + 4 * NB + 10 * NB + 4 * NFX + 4 * NGY;
-    static constexpr size_t bytes = sizeof(double) * (size_t)doubles;
+    static constexpr int words = 12 * NB + 4 * NB + 10 * NB + 4 * NFX + 4 * NGY;
+    static constexpr size_t bytes = sizeof(R) * (size_t)words;
 };
 
 #ifndef CHAN_MINB
-#define CHAN_MINB 2   // resident CTAs per SM the register budget is sized for
+#define CHAN_MINB 2   // resident CTAs per SM the register budget is sized for (FP64 rings)
+#endif
+#ifndef CHAN_MINB_F
+#define CHAN_MINB_F 3 // the same with float rings (half the shared memory)
 #endif
 
-template <int TI, int TJ>
-__global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
+template <typename R>
+__device__ __forceinline__ const FluxC<R> &fluxc(const KParams &P);
+template <>
+__device__ __forceinline__ const FluxC<double> &fluxc<double>(const KParams &P) { return P.cd; }
+template <>
+__device__ __forceinline__ const FluxC<float> &fluxc<float>(const KParams &P) { return P.cf; }
+
+// per-k tables: 0 czh, 1 cz8, 2 cz12, 3 pez
+template <typename R>
+__device__ __forceinline__ R ktab(const KParams &P, int which, int k);
+template <>
+__device__ __forceinline__ double ktab<double>(const KParams &P, int which, int k)
 {
-    using S = StageShape<TI, TJ>;
+    return which == 0 ? P.czh[k] : (which == 1 ? P.cz8[k] : (which == 2 ? P.cz12[k] : P.pez[k]));
+}
+template <>
+__device__ __forceinline__ float ktab<float>(const KParams &P, int which, int k)
+{
+    return P.tabf[which * (P.n3 + 2) + k];
+}
+
+// mu = T^0.7 in the ring type: pow07 in double; exp2(0.7 log2 T) in float
+template <typename R>
+__device__ __forceinline__ R mu_of(double T);
+template <>
+__device__ __forceinline__ double mu_of<double>(double T) { return pow07(T); }
+template <>
+__device__ __forceinline__ float mu_of<float>(double T) { return exp2f(0.7f * log2f((float)T)); }
+
+template <typename T>
+__device__ __forceinline__ double ldq(const T *p) { return (double)__ldg(p); }
+
+template <int TI, int TJ, typename QI, typename QO, typename R>
+__global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MINB) k_stage(const KParams P)
+{
+    using S = StageShape<TI, TJ, R>;
+    using Slot = SlotT<R>;
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT;
     static_assert(2 * TJ <= 32 && 32 + 2 * TI <= NT, "halo-flux lane layout needs 2*TJ <= 32 and 32+2*TI <= TI*TJ");
-    extern __shared__ double smem[];
-    double *sPr = smem;            // [3][4][NB]
-    double *sMP = sPr + 12 * NB;   // [2][2][NB]   mu, p
-    double *sQ = sMP + 4 * NB;     // [2][5][NB]
-    double *sF = sQ + 10 * NB;     // [4][TJ][TI+2]
-    double *sG = sF + 4 * S::NFX;  // [4][TJ+2][TI]
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *sPr = reinterpret_cast<R *>(smem_raw);   // [3][4][NB]
+    R *sMP = sPr + 12 * NB;                     // [2][2][NB]   mu, p
+    R *sQ = sMP + 4 * NB;                       // [2][5][NB]
+    R *sF = sQ + 10 * NB;                       // [4][TJ][TI+2]
+    R *sG = sF + 4 * S::NFX;                    // [4][TJ+2][TI]
     __shared__ int s_frozen;
+    const FluxC<R> &C = fluxc<R>(P);
+    // the state pointers are read from the parameter space at each use: held
+    // in registers across the kernel they cost spills
+    auto qin = [&]() { return static_cast<const QI *>(P.qin); };
+    auto qout = [&]() { return static_cast<QO *>(P.qout); };
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
     if (tid == 0) s_frozen = frozen(P.status, P.step) ? 1 : 0;
@@ -379,7 +446,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 
     // ring slots by role, rotated once per plane instead of indexed by plane:
     // prims (u,v,w,T) for t-1, t, t+1 at offsets oM, oZ, oP; Q and (mu,p) for
-    // t, t+1 at qZ, qP and mZ, mP (offsets in doubles)
+    // t, t+1 at qZ, qP and mZ, mP (offsets in words)
     int oM = 0, oZ = 4 * NB, oP = 8 * NB, qZ = 0, qP = 5 * NB, mZ = 0, mP = 2 * NB;
     auto slot = [&](int o) -> Slot {
         return Slot{sPr + o, sPr + o + NB, sPr + o + 2 * NB, sPr + o + 3 * NB};
@@ -415,7 +482,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     // values from memory instead (hflux_wall).
     auto load_plane = [&](int m, int po, int qo, int mo) {
         const Slot s = slot(po);
-        double *MU = smu(mo), *PR = spr(mo);
+        R *MU = smu(mo), *PR = spr(mo);
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
 #pragma unroll
@@ -426,10 +493,11 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             double q[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                q[v] = __ldg(P.qin + v * vol + off);
-                sq(qo, v)[p] = q[v];
+                q[v] = ldq(qin() + v * vol + off);
+                sq(qo, v)[p] = (R)q[v];
             }
-            double u, vv, w, T, mu, pr;
+            double u, vv, w, T, pr;
+            R mu;
             if (wall) {
                 const int bj = p / BX, bi = p - bj * BX;
                 const long long wo = (long long)wrap_idx(j0 - 2 + bj, n2) * P.px + wrap_idx(i0 - 2 + bi, n1);
@@ -438,18 +506,18 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 w = W[3 * plane + wo];
                 T = W[5 * plane + wo];
                 pr = W[6 * plane + wo];
-                mu = W[7 * plane + wo];
+                mu = (R)W[7 * plane + wo];
             } else {
                 prims_from_q(P, q, u, vv, w, T);
                 pr = (q[0] * T) * P.inv_gM2;
-                mu = (lp[l] & 0x10000) ? pow07(T) : 0.0;
+                mu = (lp[l] & 0x10000) ? mu_of<R>(T) : R(0);
             }
-            ((double *)s.U)[p] = u;
-            ((double *)s.V)[p] = vv;
-            ((double *)s.W)[p] = w;
-            ((double *)s.T)[p] = T;
+            ((R *)s.U)[p] = (R)u;
+            ((R *)s.V)[p] = (R)vv;
+            ((R *)s.W)[p] = (R)w;
+            ((R *)s.T)[p] = (R)T;
             MU[p] = mu;
-            PR[p] = pr;
+            PR[p] = (R)pr;
         }
     };
 
@@ -457,7 +525,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     auto center = [&](int m, double q[5], double &u, double &v, double &w, double &T) {
         const long long off = (long long)m * plane + colo;
 #pragma unroll
-        for (int c = 0; c < 5; c++) q[c] = __ldg(P.qin + c * vol + off);
+        for (int c = 0; c < 5; c++) q[c] = ldq(qin() + c * vol + off);
         if (m == 1 || m == n3) {
             const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane + colo;
             u = W[1 * plane]; v = W[2 * plane]; w = W[3 * plane]; T = W[5 * plane];
@@ -467,17 +535,16 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     };
 
     // hD at the own column of interior plane m (in ring); dz from (m-1, m+1) values
-    auto hflux = [&](int m, int po, int mo, double um, double vm, double wm, double Tm, double up, double vp,
-                     double wp_, double Tp, double h[4]) {
+    auto hflux = [&](int m, int po, int mo, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
         const Slot s = slot(po);
-        const double sc = P.czh[m];
-        visc_fz<BX>(P, s, smu(mo)[bc], spr(mo)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
+        const R sc = ktab<R>(P, 0, m);
+        visc_fz<BX>(C, s, smu(mo)[bc], spr(mo)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
                     (Tp - Tm) * sc, h);
     };
     // hD at the own column of wall plane m, from the wall's own values in
-    // memory; one-sided dz against the interior neighbour values (ui..Ti):
-    // (q(2)-q(1))/dz1 at the bottom, (q(nP3)-q(nP3-1))/dzN at the top.  The
-    // pressure is the pressure-BC state.
+    // memory, in double; one-sided dz against the interior neighbour values
+    // (ui..Ti): (q(2)-q(1))/dz1 at the bottom, (q(nP3)-q(nP3-1))/dzN at the
+    // top.  The pressure is the pressure-BC state.
     auto hflux_wall = [&](int m, double ui, double vi, double wi, double Ti, double h[4]) {
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane + colo;
         const long long px = P.px;
@@ -489,12 +556,12 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         const double wy = (W[3 * plane + px] - W[3 * plane - px]) * P.hdy;
         const double uz = (m == 1 ? ui - u0 : u0 - ui) * sc, vz = (m == 1 ? vi - v0 : v0 - vi) * sc;
         const double wz = (m == 1 ? wi - w0 : w0 - wi) * sc, Tz = (m == 1 ? Ti - T0 : T0 - Ti) * sc;
-        visc_fz_vals(P, ux, vy, wx, wy, u0, v0, w0, W[7 * plane], W[6 * plane], uz, vz, wz, Tz, h);
+        visc_fz_vals(P.cd, ux, vy, wx, wy, u0, v0, w0, W[7 * plane], W[6 * plane], uz, vz, wz, Tz, h);
     };
 
     // ---------------- prologue: planes kb-1 and kb, hD(kb-1), hD(kb)
-    double qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
-    double wm2 = 0.0;
+    R qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
+    R wm2 = R(0);
     load_plane(kb - 1, oM, qP, mP);
     load_plane(kb, oZ, qZ, mZ);
     __syncthreads();
@@ -503,22 +570,27 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         if (col_ok) {
             // hD(kb-1)
             if (kb - 1 == 1) {
-                hflux_wall(1, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                double h[4];
+                hflux_wall(1, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], h);
+#pragma unroll
+                for (int c = 0; c < 4; c++) hm1[c] = (R)h[c];
             } else {
                 double q[5], u, v, w, T;
                 center(kb - 2, q, u, v, w, T);
-                hflux(kb - 1, oM, mP, u, v, w, T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                hflux(kb - 1, oM, mP, (R)u, (R)v, (R)w, (R)T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
             }
             // hD(kb)
             {
                 double q[5], u, v, w, T;
                 center(kb + 1, q, u, v, w, T);
-                hflux(kb, oZ, mZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], u, v, w, T, h0);
+                hflux(kb, oZ, mZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], (R)u, (R)v, (R)w, (R)T, h0);
             }
             if (kb - 2 >= 1) {
-                double u, v, w, T;
-                center(kb - 2, qm2, u, v, w, T);
-                wm2 = w;
+                double q[5], u, v, w, T;
+                center(kb - 2, q, u, v, w, T);
+#pragma unroll
+                for (int c = 0; c < 5; c++) qm2[c] = (R)q[c];
+                wm2 = (R)w;
             }
             // the last chunk stages hD of the top wall plane for its last plane
             if (ke == n3 - 1) {
@@ -532,7 +604,7 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             for (int c = 0; c < 5; c++) qm1[c] = sq(qP, c)[bc];
         } else {
 #pragma unroll
-            for (int c = 0; c < 5; c++) qm1[c] = 0.0;
+            for (int c = 0; c < 5; c++) qm1[c] = R(0);
         }
     }
     __syncthreads();
@@ -540,22 +612,27 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
     for (int t = kb; t <= ke; t++) {
         // ---------- A: plane t+1 into the ring; own column of t+2
         load_plane(t + 1, oP, qP, mP);
-        double qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
-        if (col_ok && t + 2 <= n3) center(t + 2, qp2, up2, vp2, wp2, Tp2);
+        R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
+        if (col_ok && t + 2 <= n3) {
+            double q[5], u, v, w, T;
+            center(t + 2, q, u, v, w, T);
+#pragma unroll
+            for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
+            up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
+        }
         __syncthreads();
 
         // ---------- C: viscous flux vectors
         const Slot s0 = slot(oZ), sm = slot(oM), sp = slot(oP);
-        double hp1[4] = {0, 0, 0, 0};
-        // RK base state of the own point, fetched early (stages that use it)
+        R hp1[4] = {0, 0, 0, 0};
         {
-            const double czt = P.czh[t];
-            const double *MU = smu(mZ), *PR = spr(mZ);
+            const R czt = ktab<R>(P, 0, t);
+            const R *MU = smu(mZ), *PR = spr(mZ);
             if (col_ok) {
                 if (t + 1 != n3)
                     hflux(t + 1, oP, mP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
-                double f[4], g[4];
-                visc_fxy<BX>(P, s0, sm, sp, MU, PR, bc, czt, f, g);
+                R f[4], g[4];
+                visc_fxy<BX>(C, s0, sm, sp, MU, PR, bc, czt, f, g);
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
                     sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
@@ -568,8 +645,8 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 const int side = tid / TJ, r = tid - side * TJ;
                 const int ci = side ? i0 + TI : i0 - 1, cj = j0 + r;
                 if (ci <= n1 && cj <= n2) {
-                    double f[4];
-                    visc_fx<BX>(P, s0, sm, sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1), czt, f);
+                    R f[4];
+                    visc_fx<BX>(C, s0, sm, sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1), czt, f);
 #pragma unroll
                     for (int c = 0; c < 4; c++) sF[(c * TJ + r) * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
                 }
@@ -577,8 +654,8 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
                 const int h = tid - 32, side = h / TI, cc = h - side * TI;
                 const int ci = i0 + cc, cj = side ? j0 + TJ : j0 - 1;
                 if (ci <= n1 && cj <= n2) {
-                    double g[4];
-                    visc_fy<BX>(P, s0, sm, sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2, czt, g);
+                    R g[4];
+                    visc_fy<BX>(C, s0, sm, sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2, czt, g);
 #pragma unroll
                     for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + (side ? TJ + 1 : 0)) * TI + cc] = g[c];
                 }
@@ -587,89 +664,99 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
         __syncthreads();
 
         // ---------- E: fluxes, source, RK update
-        double q0[5];
+        R q0[5];
 #pragma unroll
         for (int c = 0; c < 5; c++) q0[c] = sq(qZ, c)[bc];
-        const double wm1 = sm.W[bc];
+        const R wm1 = sm.W[bc];
         if (out_ok) {
-            double R[5];
-            const double mu0 = smu(mZ)[bc];
+            R Fs[5];   // sum of the flux derivatives
+            const R mu0 = smu(mZ)[bc];
             // x
             {
-                const double *U = s0.U;
-                const bool qk = (P.pex * fabs(q0[1])) > P.PexVal * mu0;
-                double w[5];
-                inv_weights(U[bc - 2], U[bc - 1], U[bc], U[bc + 1], U[bc + 2], qk, P.sx8, P.sx12, w);
-                double F1[5];
+                const R *U = s0.U;
+                const bool qk = (C.pex * fabs(q0[1])) > C.PexVal * mu0;
+                R w[5];
+                inv_weights(U[bc - 2], U[bc - 1], U[bc], U[bc + 1], U[bc + 2], qk, C.sx8, C.sx12, w);
+                R F1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const double *Q = sq(qZ, c);
+                    const R *Q = sq(qZ, c);
                     F1[c] = wsum(w, Q[bc - 2], Q[bc - 1], Q[bc], Q[bc + 1], Q[bc + 2]);
                 }
-                R[0] = F1[0];  // F2 of continuity is zero
+                Fs[0] = F1[0];  // F2 of continuity is zero
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
                     const int r = (c - 1) * TJ + ty;
-                    const double F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * P.hdx;
-                    R[c] = F1[c] + F2;
+                    const R F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * C.hdx;
+                    Fs[c] = F1[c] + F2;
                 }
             }
             // y
             {
-                const double *V = s0.V;
-                const bool qk = (P.pey * fabs(q0[2])) > P.PeyVal * mu0;
-                double w[5];
-                inv_weights(V[bc - 2 * BX], V[bc - BX], V[bc], V[bc + BX], V[bc + 2 * BX], qk, P.sy8, P.sy12, w);
-                double G1[5];
+                const R *V = s0.V;
+                const bool qk = (C.pey * fabs(q0[2])) > C.PeyVal * mu0;
+                R w[5];
+                inv_weights(V[bc - 2 * BX], V[bc - BX], V[bc], V[bc + BX], V[bc + 2 * BX], qk, C.sy8, C.sy12, w);
+                R G1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const double *Q = sq(qZ, c);
+                    const R *Q = sq(qZ, c);
                     G1[c] = wsum(w, Q[bc - 2 * BX], Q[bc - BX], Q[bc], Q[bc + BX], Q[bc + 2 * BX]);
                 }
-                R[0] = R[0] + G1[0];
+                Fs[0] = Fs[0] + G1[0];
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const double G2 = (sG[((c - 1) * (TJ + 2) + ty + 2) * TI + tx] -
-                                       sG[((c - 1) * (TJ + 2) + ty) * TI + tx]) * P.hdy;
-                    R[c] = (R[c] + G1[c]) + G2;
+                    const R G2 = (sG[((c - 1) * (TJ + 2) + ty + 2) * TI + tx] -
+                                  sG[((c - 1) * (TJ + 2) + ty) * TI + tx]) * C.hdy;
+                    Fs[c] = (Fs[c] + G1[c]) + G2;
                 }
             }
             // z
             {
-                const double w0 = s0.W[bc], wp1 = sp.W[bc];
-                double w[5];
+                const R w0 = s0.W[bc], wp1 = sp.W[bc];
+                R w[5];
                 if (t < 3 || t > n3 - 2) {
-                    const double c2 = P.czh[t];
-                    w[0] = 0.0; w[1] = -(wm1 * c2); w[2] = 0.0; w[3] = wp1 * c2; w[4] = 0.0;
+                    const R c2 = ktab<R>(P, 0, t);
+                    w[0] = R(0); w[1] = -(wm1 * c2); w[2] = R(0); w[3] = wp1 * c2; w[4] = R(0);
                 } else {
-                    const bool qk = (P.pez[t] * fabs(q0[3])) > P.pez_val * mu0;
-                    inv_weights(wm2, wm1, w0, wp1, wp2, qk, P.cz8[t], P.cz12[t], w);
+                    const bool qk = (ktab<R>(P, 3, t) * fabs(q0[3])) > C.pez_val * mu0;
+                    inv_weights(wm2, wm1, w0, wp1, wp2, qk, ktab<R>(P, 1, t), ktab<R>(P, 2, t), w);
                 }
-                const double czt = P.czh[t];
-                R[0] = R[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(qP, 0)[bc], qp2[0]);
+                const R czt = ktab<R>(P, 0, t);
+                Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(qP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const double H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(qP, c)[bc], qp2[c]);
-                    const double hp = top ? P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
-                    const double H2 = (hp - hm1[c - 1]) * czt;
-                    R[c] = (R[c] + H1) + H2;
+                    const R H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(qP, c)[bc], qp2[c]);
+                    const R hp = top ? (R)P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
+                    const R H2 = (hp - hm1[c - 1]) * czt;
+                    Fs[c] = (Fs[c] + H1) + H2;
                 }
             }
-            // source: lagged wall-shear forcing (main_v1.9.f90:565-571)
+            // source: lagged wall-shear forcing (main_v1.9.f90:565-571), in double
             double src2 = 0.0, src5 = 0.0;
             if (P.force_on) {
                 const double tau = P.stat[23 * n3 + 0] - P.stat[23 * n3 + 1];
                 const double rb = P.stat[t - 1];
                 src2 = (0.5 * tau) * rb;
-                src5 = (((P.ggM * s0.U[bc]) * 0.5) * tau) * rb;
+                src5 = (((P.ggM * (double)s0.U[bc]) * 0.5) * tau) * rb;
             }
-            R[0] = -R[0];
-            R[1] = src2 - R[1];
-            R[2] = -R[2];
-            R[3] = -R[3];
-            R[4] = src5 - R[4];
-            // RK update
+            double Rd[5];
+            Rd[0] = -(double)Fs[0];
+            Rd[1] = src2 - (double)Fs[1];
+            Rd[2] = -(double)Fs[2];
+            Rd[3] = -(double)Fs[3];
+            Rd[4] = src5 - (double)Fs[4];
+            // RK update in double, on the stage input at its stored precision
+            double qs[5];
+            if (std::is_same<QI, R>::value) {
+#pragma unroll
+                for (int c = 0; c < 5; c++) qs[c] = (double)q0[c];
+            } else {
+                const long long off = (long long)t * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) qs[c] = ldq(qin() + c * vol + off);
+            }
             double qn[5];
             double qb[5] = {0, 0, 0, 0, 0};
             if (P.rk_mode != 0) {
@@ -679,13 +766,13 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             }
             if (P.rk_mode == 0) {
 #pragma unroll
-                for (int c = 0; c < 5; c++) qn[c] = q0[c] + P.rk_cdt * R[c];
+                for (int c = 0; c < 5; c++) qn[c] = qs[c] + P.rk_cdt * Rd[c];
             } else if (P.rk_mode == 1) {
 #pragma unroll
-                for (int c = 0; c < 5; c++) qn[c] = qb[c] + P.rk_cdt * R[c];
+                for (int c = 0; c < 5; c++) qn[c] = qb[c] + P.rk_cdt * Rd[c];
             } else {
 #pragma unroll
-                for (int c = 0; c < 5; c++) qn[c] = (P.rk_a * qb[c] + P.rk_b * q0[c]) + P.rk_cdt * R[c];
+                for (int c = 0; c < 5; c++) qn[c] = (P.rk_a * qb[c] + P.rk_b * qs[c]) + P.rk_cdt * Rd[c];
             }
             // store + periodic images (the ghosts the reference's halo exchange fills)
             const int im = (i <= 3) ? i + (n1 - 2) : ((i >= n1 - 2) ? i - (n1 - 2) : -1);
@@ -693,11 +780,12 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
             const long long pk = (long long)t * plane;
 #pragma unroll
             for (int c = 0; c < 5; c++) {
-                double *O = P.qout + c * vol + pk;
-                O[(long long)j * P.px + i] = qn[c];
-                if (im >= 0) O[(long long)j * P.px + im] = qn[c];
-                if (jm >= 0) O[(long long)jm * P.px + i] = qn[c];
-                if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = qn[c];
+                QO *O = qout() + c * vol + pk;
+                const QO v = (QO)qn[c];
+                O[(long long)j * P.px + i] = v;
+                if (im >= 0) O[(long long)j * P.px + im] = v;
+                if (jm >= 0) O[(long long)jm * P.px + i] = v;
+                if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = v;
             }
             if (P.check) {
                 const double tr = qn[0] * qn[4] - P.ggMh * ((qn[1] * qn[1] + qn[2] * qn[2]) + qn[3] * qn[3]);
@@ -736,8 +824,10 @@ __global__ void __launch_bounds__(TI *TJ, CHAN_MINB) k_stage(const KParams P)
 
 // var(u, v, T) of an interior point as the reference holds it (corner columns
 // keep their stale values)
+template <typename QT>
 __device__ __forceinline__ void inner_uvT(const KParams &P, int i, int j, int k, double &u, double &v, double &T)
 {
+    const QT *qo = static_cast<const QT *>(P.qout);
     const int n1 = P.n1, n2 = P.n2;
     if ((i == 1 || i == n1) && (j == 1 || j == n2)) {
         const double *C = P.cs + ((size_t)k * 4 + (i == 1 ? 0 : 1) + (j == 1 ? 0 : 2)) * 7;
@@ -745,15 +835,16 @@ __device__ __forceinline__ void inner_uvT(const KParams &P, int i, int j, int k,
         return;
     }
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
-    const double q0 = P.qout[o];
-    u = P.qout[P.vol + o] / q0;
-    v = P.qout[2 * P.vol + o] / q0;
-    const double w = P.qout[3 * P.vol + o] / q0;
-    const double E = P.qout[4 * P.vol + o] / q0;
+    const double q0 = qo[o];
+    u = (double)qo[P.vol + o] / q0;
+    v = (double)qo[2 * P.vol + o] / q0;
+    const double w = (double)qo[3 * P.vol + o] / q0;
+    const double E = (double)qo[4 * P.vol + o] / q0;
     T = E - P.ggMh * ((u * u + v * v) + w * w);
 }
 
 // wall values u, v, T of point (i,j) of wall `wall` after the wall BC
+template <typename QT>
 __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, double &v, double &T)
 {
     const WallBC &B = P.wbc[wall];
@@ -766,8 +857,8 @@ __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, 
     double u2 = 0, v2 = 0, T2 = 0, u3 = 0, v3 = 0, T3 = 0;
     const bool need_inner = (B.vel == 1 && B.mask[(jc - 1) * n1 + ic - 1]) || B.therm == 1;
     if (need_inner) {
-        inner_uvT(P, ic, jc, k2, u2, v2, T2);
-        inner_uvT(P, ic, jc, k3, u3, v3, T3);
+        inner_uvT<QT>(P, ic, jc, k2, u2, v2, T2);
+        inner_uvT<QT>(P, ic, jc, k3, u3, v3, T3);
     }
     if (B.vel == 1) {
         if (B.mask[(jc - 1) * n1 + ic - 1]) {
@@ -784,8 +875,11 @@ __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, 
     T = (B.therm == 1) ? ((B.dTdz - c[1] * T2) - c[2] * T3) / c[0] : B.Tw;
 }
 
+// QT: storage type of the stage output the wall BC reads (the planes next to the wall)
+template <typename QT>
 __global__ void k_wall(const KParams P)
 {
+    const QT *qo = static_cast<const QT *>(P.qout);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int wall = blockIdx.z;
@@ -799,7 +893,7 @@ __global__ void k_wall(const KParams P)
     double uw = 0.0, vw = 0.0, Tw = wall == 0 ? P.Twb : P.Twt;
     double muw = wall == 0 ? P.muwb : P.muwt;
     if (custom) {
-        wall_point(P, wall, i, j, uw, vw, Tw);
+        wall_point<QT>(P, wall, i, j, uw, vw, Tw);
         if (P.wbc[wall].therm == 1) muw = pow07(Tw);
     }
     const double pold = W[6 * plane + idx];
@@ -814,8 +908,8 @@ __global__ void k_wall(const KParams P)
         auto prim = [&](int ii, int jj, int kk, double &r, double &u, double &v, double &w, double &T,
                         double &p, double &mu) {
             const long long o = (long long)kk * plane + (long long)jj * P.px + ii;
-            const double q0 = P.qout[o], q1 = P.qout[vol + o], q2 = P.qout[2 * vol + o];
-            const double q3 = P.qout[3 * vol + o], q4 = P.qout[4 * vol + o];
+            const double q0 = qo[o], q1 = qo[vol + o], q2 = qo[2 * vol + o];
+            const double q3 = qo[3 * vol + o], q4 = qo[4 * vol + o];
             r = q0;
             u = q1 / q0; v = q2 / q0; w = q3 / q0;
             const double E = q4 / q0;
@@ -827,13 +921,13 @@ __global__ void k_wall(const KParams P)
         double t_ip = 0.0, t_im = 0.0, t_jp = 0.0, t_jm = 0.0;
         if (custom) {
             double u, v, T;
-            wall_point(P, wall, i + 1, j, u, v, T);
+            wall_point<QT>(P, wall, i + 1, j, u, v, T);
             t_ip = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * u;
-            wall_point(P, wall, i - 1, j, u, v, T);
+            wall_point<QT>(P, wall, i - 1, j, u, v, T);
             t_im = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * u;
-            wall_point(P, wall, i, j + 1, u, v, T);
+            wall_point<QT>(P, wall, i, j + 1, u, v, T);
             t_jp = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * v;
-            wall_point(P, wall, i, j - 1, u, v, T);
+            wall_point<QT>(P, wall, i, j - 1, u, v, T);
             t_jm = c1[0] * (P.wbc[wall].therm == 1 ? pow07(T) : muw) * v;
         }
         double r, u, v, w, T, p, mu;
@@ -1288,6 +1382,13 @@ __global__ void k_check(const KParams P, const double *q)
         ref_var(P, q, ii + 1, jj + 1, kk + 1, x);
         if (x[0] < 0.0 || x[5] < 0.0) flag_blown(P.status, ii + 1, jj + 1, kk + 1, P.step);
     }
+}
+
+// double -> float copy (seeds the mixed-precision stage buffers)
+__global__ void k_to_float(const double *a, float *b, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
 }
 
 // self-test of pow07 against the CUDA math library's pow (diagnostics only)

@@ -41,7 +41,10 @@ struct chan_ctx {
     int dev = 0;
     cudaStream_t stream = nullptr;
     chan::KParams kp{};
-    double *q[3] = {nullptr, nullptr, nullptr};
+    double *q[3] = {nullptr, nullptr, nullptr};   // plain FP64: state and two stage buffers
+    float *qf[2] = {nullptr, nullptr};            // mixed precision: the two stage buffers in float
+    bool mixed = false;
+    float *tabf = nullptr;                        // per-k tables in float (mixed)
     double *wp = nullptr, *cs = nullptr, *tabs = nullptr, *stat = nullptr, *dvar = nullptr, *tacc = nullptr;
     double *hwt = nullptr;   // hD of the top wall plane, staged inside a stage
     double *spart = nullptr; // statistics partial sums [(nP3+2)*nsplit][23]
@@ -164,25 +167,29 @@ void set_stage(chan_ctx *c, int iter)
 {
     chan::KParams &k = c->kp;
     const double dt = c->p.dt;
+    // stage buffers: B and C are q[1], q[2] (FP64) or qf[0], qf[1] (mixed precision)
+    void *A = c->q[0];
+    void *B = c->mixed ? (void *)c->qf[0] : (void *)c->q[1];
+    void *Cb = c->mixed ? (void *)c->qf[1] : (void *)c->q[2];
     if (c->nstage == 3) {
         if (iter == 1) {
-            k.qin = c->q[0]; k.qbase = c->q[0]; k.qout = c->q[1];
+            k.qin = A; k.qbase = c->q[0]; k.qout = B;
             k.rk_mode = 0; k.rk_a = 0.0; k.rk_b = 1.0; k.rk_cdt = dt;
         } else if (iter == 2) {
-            k.qin = c->q[1]; k.qbase = c->q[0]; k.qout = c->q[2];
+            k.qin = B; k.qbase = c->q[0]; k.qout = Cb;
             k.rk_mode = 2; k.rk_a = 0.75; k.rk_b = 0.25; k.rk_cdt = 0.25 * dt;
         } else {
-            k.qin = c->q[2]; k.qbase = c->q[0]; k.qout = c->q[0];
+            k.qin = Cb; k.qbase = c->q[0]; k.qout = A;
             k.rk_mode = 2; k.rk_a = 1.0 / 3.0; k.rk_b = 2.0 / 3.0; k.rk_cdt = (2.0 / 3.0) * dt;
         }
     } else {
         if (iter == 1) {
             // solV(:,2)=solV(:,1); solV(:,1)+=haf*dt*R  (main_v1.9.f90:575-578)
-            k.qin = c->q[0]; k.qbase = c->q[0]; k.qout = c->q[1];
+            k.qin = A; k.qbase = c->q[0]; k.qout = B;
             k.rk_mode = 0; k.rk_a = 0.0; k.rk_b = 1.0; k.rk_cdt = 0.5 * dt;
         } else {
             // solV(:,1)=solV(:,2)+dt*R  (main_v1.9.f90:580-582)
-            k.qin = c->q[1]; k.qbase = c->q[0]; k.qout = c->q[0];
+            k.qin = B; k.qbase = c->q[0]; k.qout = A;
             k.rk_mode = 1; k.rk_a = 1.0; k.rk_b = 0.0; k.rk_cdt = dt;
         }
     }
@@ -192,21 +199,47 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
 {
     set_stage(c, iter);
     c->kp.time = time;
-    c->cur = c->kp.qout == c->q[0] ? 0 : (c->kp.qout == c->q[1] ? 1 : 2);
+    c->cur = c->kp.qout == (void *)c->q[0] ? 0 : (c->kp.qout == (void *)c->q[1] ? 1 : 2);
     c->kp.check = check ? 1 : 0;
     c->kp.step = step;
+    const bool last = iter == c->nstage;
     {
         ProfScope ps(c, 0);
         dim3 grid(c->ntx, c->nty, c->nchunks), block(TI, TJ);
-        chan::k_stage<TI, TJ><<<grid, block, chan::StageShape<TI, TJ>::bytes, c->stream>>>(c->kp);
+        const size_t smf = chan::StageShape<TI, TJ, float>::bytes;
+        if (!c->mixed)
+            chan::k_stage<TI, TJ, double, double, double>
+                <<<grid, block, chan::StageShape<TI, TJ, double>::bytes, c->stream>>>(c->kp);
+        else if (iter == 1)
+            chan::k_stage<TI, TJ, double, float, float><<<grid, block, smf, c->stream>>>(c->kp);
+        else if (last)
+            chan::k_stage<TI, TJ, float, double, float><<<grid, block, smf, c->stream>>>(c->kp);
+        else
+            chan::k_stage<TI, TJ, float, float, float><<<grid, block, smf, c->stream>>>(c->kp);
     }
     CK(c, cudaGetLastError());
     {
         ProfScope ps(c, 1);
         dim3 block(32, 8), grid((c->n1 + 2 + 31) / 32, (c->n2 + 2 + 7) / 8, 2);
-        chan::k_wall<<<grid, block, 0, c->stream>>>(c->kp);
+        if (c->mixed && !last)
+            chan::k_wall<float><<<grid, block, 0, c->stream>>>(c->kp);
+        else
+            chan::k_wall<double><<<grid, block, 0, c->stream>>>(c->kp);
     }
     CK(c, cudaGetLastError());
+    return CHAN_OK;
+}
+
+// mixed precision: the float stage buffers start as copies of the state, so
+// their wall planes and wall ghosts (which no stage writes) hold the state's
+int seed_float_stages(chan_ctx *c)
+{
+    if (!c->mixed) return CHAN_OK;
+    const long long n = 5 * c->vol;
+    for (int b = 0; b < 2; b++) {
+        chan::k_to_float<<<1184, 256, 0, c->stream>>>(c->q[0], c->qf[b], n);
+        CK(c, cudaGetLastError());
+    }
     return CHAN_OK;
 }
 
@@ -439,7 +472,7 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     }
     if (p->rk_scheme != CHAN_RK2 && p->rk_scheme != CHAN_RK3) { g_init_error = "rk_scheme must be 2 or 3"; return CHAN_EINVAL; }
     if (p->forcing != CHAN_FORCE_WALLSHEAR && p->forcing != CHAN_FORCE_NONE) { g_init_error = "bad forcing"; return CHAN_EINVAL; }
-    if (p->flags != 0) { g_init_error = "flags must be 0"; return CHAN_EINVAL; }
+    if ((p->flags & ~CHAN_MIXED) != 0) { g_init_error = "flags must be 0 or CHAN_MIXED"; return CHAN_EINVAL; }
     if (p->istat < 0) { g_init_error = "istat must be >= 0"; return CHAN_EINVAL; }
     for (int k = 1; k < p->nP[2]; k++)
         if (!(x3[k] > x3[k - 1])) { g_init_error = "x3 must increase"; return CHAN_EINVAL; }
@@ -461,9 +494,20 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     c->nstage = p->rk_scheme == CHAN_RK3 ? 3 : 2;
     c->hx3.assign(x3, x3 + n3);
 
+    c->mixed = (p->flags & CHAN_MIXED) != 0;
     int r;
-    for (int b = 0; b < 3; b++)
+    for (int b = 0; b < (c->mixed ? 1 : 3); b++)
         if ((r = dalloc(c, &c->q[b], 5 * (size_t)c->vol))) { g_init_error = c->err; chan_free(c); return r; }
+    if (c->mixed) {
+        for (int b = 0; b < 2; b++) {
+            double *t = nullptr;
+            if ((r = dalloc(c, &t, (5 * (size_t)c->vol + 1) / 2))) { g_init_error = c->err; chan_free(c); return r; }
+            c->qf[b] = reinterpret_cast<float *>(t);
+        }
+        double *t = nullptr;
+        if ((r = dalloc(c, &t, (4 * (size_t)(n3 + 2) + 1) / 2))) { g_init_error = c->err; chan_free(c); return r; }
+        c->tabf = reinterpret_cast<float *>(t);
+    }
     if ((r = dalloc(c, &c->wp, 2 * 8 * (size_t)c->plane)) || (r = dalloc(c, &c->cs, (size_t)(n3 + 2) * 28)) ||
         (r = dalloc(c, &c->tabs, 4 * (size_t)(n3 + 2))) || (r = dalloc(c, &c->stat, 23 * (size_t)n3 + 2)) ||
         (r = dalloc(c, &c->tacc, 23 * (size_t)n3 + 2)) || (r = dalloc(c, &c->hwt, 4 * (size_t)c->plane)) ||
@@ -495,6 +539,10 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
         tab[3 * (n3 + 2) + k] = (Re * dXi) * JAC[k];
     }
     e = cudaMemcpyAsync(c->tabs, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    std::vector<float> tabf(tab.begin(), tab.end());
+    if (e == cudaSuccess && c->mixed)
+        e = cudaMemcpyAsync(c->tabf, tabf.data(), tabf.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { fail(nullptr, "table upload", e); chan_free(c); return CHAN_ECUDA; }
 
     chan::KParams &k = c->kp;
@@ -517,6 +565,13 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     k.pex = Re * dx; k.pey = Re * dy;
     k.PexVal = p->Pe[0]; k.PeyVal = p->Pe[1]; k.pez_val = p->Pe[2];
     k.inv_dz1 = 1.0 / co[12]; k.inv_dzN = 1.0 / co[13];
+    k.tabf = c->tabf;
+    k.cd = chan::FluxC<double>{k.invRe, k.ggM, k.two3rd, k.kq, k.inv_gM2, k.hdx, k.hdy, k.sx8, k.sx12, k.sy8,
+                               k.sy12, k.pex, k.pey, k.PexVal, k.PeyVal, k.pez_val};
+    k.cf = chan::FluxC<float>{(float)k.invRe, (float)k.ggM, (float)k.two3rd, (float)k.kq, (float)k.inv_gM2,
+                              (float)k.hdx, (float)k.hdy, (float)k.sx8, (float)k.sx12, (float)k.sy8,
+                              (float)k.sy12, (float)k.pex, (float)k.pey, (float)k.PexVal, (float)k.PeyVal,
+                              (float)k.pez_val};
     k.Twb = p->Tw[0]; k.Twt = p->Tw[1];
     k.muwb = pow(p->Tw[0], 0.7); k.muwt = pow(p->Tw[1], 0.7);
     for (int m = 0; m < 3; m++) {
@@ -532,12 +587,26 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     // stage-kernel launch shape: tiles x k-chunks filling whole waves
     c->ntx = (n1 - 2 + TI - 1) / TI;
     c->nty = (n2 - 2 + TJ - 1) / TJ;
-    const size_t smem = chan::StageShape<TI, TJ>::bytes;
-    e = cudaFuncSetAttribute(chan::k_stage<TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = chan::StageShape<TI, TJ, double>::bytes, smemf = chan::StageShape<TI, TJ, float>::bytes;
+    e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, double, double, double>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, double, float, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, float, float, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, float, double, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
     if (e != cudaSuccess) { fail(nullptr, "cudaFuncSetAttribute", e); chan_free(c); return CHAN_ECUDA; }
     int sms = 148, occ = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ>, TI * TJ, smem);
+    if (c->mixed)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ, float, float, float>, TI * TJ, smemf);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ, double, double, double>, TI * TJ,
+                                                      smem);
     if (occ < 1) occ = 1;
     const long long slots = (long long)sms * occ;
     const int nz = n3 - 2;
@@ -570,7 +639,8 @@ int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time)
     CK(c, cudaSetDevice(c->dev));
     const size_t N = (size_t)c->n1 * c->n2 * c->n3;
     CK(c, cudaMemcpyAsync(c->dvar, var, 7 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    chan::k_upload<<<1184, 256, 0, c->stream>>>(c->kp, c->dvar, c->q[0], c->q[1], c->q[2], c->cs);
+    chan::k_upload<<<1184, 256, 0, c->stream>>>(c->kp, c->dvar, c->q[0], c->mixed ? c->q[0] : c->q[1],
+                                                  c->mixed ? nullptr : c->q[2], c->cs);
     CK(c, cudaGetLastError());
     {
         dim3 block(32, 8), grid((c->n1 + 2 + 31) / 32, (c->n2 + 2 + 7) / 8, c->n3 - 2);
@@ -580,6 +650,7 @@ int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time)
         chan::k_fill_wall_ring<<<g2, block, 0, c->stream>>>(c->kp);
         CK(c, cudaGetLastError());
     }
+    { int r = seed_float_stages(c); if (r) return r; }
     CK(c, cudaMemsetAsync(c->stat, 0, (23 * (size_t)c->n3 + 2) * sizeof(double), c->stream));
     CK(c, cudaMemsetAsync(c->status, 0, sizeof(chan::DevStatus), c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
@@ -597,6 +668,7 @@ int chan_stage(chan_ctx *c, int iter)
     if (!c) return CHAN_EINVAL;
     if (!c->uploaded) { c->err = "chan_stage before chan_upload"; return CHAN_ESTATE; }
     if (iter < 1 || iter > c->nstage) { c->err = "iter out of range"; return CHAN_EINVAL; }
+    if (c->mixed) { c->err = "the mixed-precision path runs whole steps only (chan_step)"; return CHAN_ESTATE; }
     CK(c, cudaSetDevice(c->dev));
     int r = launch_stage(c, iter, iter == c->nstage, c->nstep + 1, c->time + c->p.dt);
     if (r) return r;
@@ -832,8 +904,9 @@ int chan_checkpoint_read(chan_ctx *c, const char *path)
     fclose(f);
     if (!ok) { c->err = std::string("checkpoint truncated: ") + path; return CHAN_EIO; }
     const double *o = hb.data();
-    for (int b = 0; b < 3; b++)
+    for (int b = 0; b < (c->mixed ? 1 : 3); b++)
         CK(c, cudaMemcpyAsync(c->q[b], o, nq * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    { int r = seed_float_stages(c); if (r) return r; }
     o += nq;
     CK(c, cudaMemcpyAsync(c->wp, o, nw * sizeof(double), cudaMemcpyHostToDevice, c->stream)); o += nw;
     CK(c, cudaMemcpyAsync(c->cs, o, ncs * sizeof(double), cudaMemcpyHostToDevice, c->stream)); o += ncs;

@@ -32,6 +32,7 @@ class ChanParams:
     rk_scheme: int = RK2
     forcing: int = FORCE_WALLSHEAR
     device: int = 0
+    mixed: bool = False           # float stage storage and fluxes, double accumulation (CHAN_MIXED)
 
     def with_(self, **kw) -> "ChanParams":
         return replace(self, **kw)

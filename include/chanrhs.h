@@ -48,6 +48,15 @@ extern "C" {
 #define CHAN_FORCE_WALLSHEAR 0  /* reference forcing 0.5*(tauL-tauU)*rhobar(k), lagged (main_v1.9.f90:547-553) */
 #define CHAN_FORCE_NONE 1       /* no source term */
 
+/* chan_params.flags: mixed precision.  The intermediate RK stage states are
+ * stored in float and the inviscid and viscous fluxes are evaluated in float;
+ * the step state, the RK accumulation against it, the temperature/pressure
+ * recovery from the total energy, the forcing, the wall BC and every
+ * reduction stay in double.  Such a context runs whole steps only
+ * (chan_stage returns CHAN_ESTATE).  The reference has no counterpart; its
+ * error against the FP64 path is measured, not bounded to 1e-12. */
+#define CHAN_MIXED 1
+
 /* Run-time parameters.  Field-for-field equivalent of the reference's
  * compile-time constants and param.dat deck (v1.9/codes/comdata.f90:4-68). */
 typedef struct chan_params {
@@ -56,7 +65,7 @@ typedef struct chan_params {
     int32_t rk_scheme;  /* CHAN_RK2 (reference) or CHAN_RK3 */
     int32_t forcing;    /* CHAN_FORCE_WALLSHEAR (reference) or CHAN_FORCE_NONE */
     int32_t device;     /* CUDA device ordinal */
-    int32_t flags;      /* reserved, must be 0 */
+    int32_t flags;      /* 0 (plain FP64) or CHAN_MIXED */
     double Re;          /* Reynolds number (param.dat) */
     double Mac;         /* Mach number (param.dat) */
     double dt;          /* time step (param.dat) */

@@ -1,0 +1,88 @@
+"""Mixed-precision path (CHAN_MIXED): float stage storage and fluxes, double
+step state, RK accumulation, T/p recovery, forcing, wall BC and reductions.
+
+Its results are not bit-parity results: the error against the FP64 oracle is
+measured and bounded here, per step, as a relative L2 norm per variable
+(||mixed - fp64|| / ||fp64|| over var(1:nP1,1:nP2,1:nP3,1:7)).
+"""
+import numpy as np
+import pytest
+
+from chan_cases import make_case
+from compchan3dmpi_b200 import Channel, ChanError, RK3
+from compchan3dmpi_b200 import wallbc as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+# relative L2 bound per variable over the first 200 steps.  v and w are the
+# small perturbation components, whose own norms decay, so their relative
+# error is also bounded against the streamwise velocity's norm.
+MIXED_TOL = np.array([1e-4, 1e-4, 1e-3, 1e-3, 1e-4, 1e-4, 1e-4])
+VEL_TOL = 1e-4
+
+
+def rel_l2(a, b):
+    return np.array([np.linalg.norm(a[m] - b[m]) / np.linalg.norm(b[m]) for m in range(a.shape[0])])
+
+
+def test_mixed_error_against_fp64_oracle_200_steps():
+    p, x3, jac, inv, var = make_case(nP=(32, 24, 33), mesh="tanh", beta=2.2, rk=RK3, Pr=0.72, istat=10, cfl=0.6)
+    g = Channel(p.with_(mixed=True), x3, jac, inv)
+    g.init_sol_v(var)
+    o = O.Oracle(p, x3, jac, inv)
+    o.upload(var)
+    worst = np.zeros(7)
+    for blk in range(20):
+        g.step(10)
+        o.step(10)
+        gv, ov = g.download(), o.download()
+        e = rel_l2(gv, ov)
+        worst = np.maximum(worst, e)
+        assert np.all(e <= MIXED_TOL), f"step {10 * (blk + 1)}: {e}"
+        un = np.linalg.norm(ov[1])
+        for m in (1, 2, 3):   # velocity errors against the streamwise velocity's norm
+            assert np.linalg.norm(gv[m] - ov[m]) / un <= VEL_TOL, (10 * (blk + 1), m)
+    assert worst.max() > 0.0          # the path really runs in reduced precision
+    gt, g1, _, _ = g.stats()
+    ot, o1, _, _ = o.stats()
+    assert np.all(np.abs(gt - ot) <= 1e-4 * np.max(np.abs(ot)))
+    for r in range(7):   # plane means against the row's scale; velocities against u's
+        scale = np.max(np.abs(o1[1])) if r in (1, 2, 3) else np.max(np.abs(o1[r]))
+        assert np.max(np.abs(g1[r] - o1[r])) <= 1e-4 * scale, r
+
+
+def test_mixed_runs_whole_steps_only_and_restarts_exactly(tmp_path):
+    p, x3, jac, inv, var = make_case(nP=(20, 14, 19), quantize=False, istat=3)
+    pm = p.with_(mixed=True)
+    a = Channel(pm, x3, jac, inv)
+    a.init_sol_v(var)
+    with pytest.raises(ChanError) as ei:
+        a.stage(1)
+    assert ei.value.code == -4
+    a.step(8)
+    ref = a.download()
+    b = Channel(pm, x3, jac, inv)
+    b.init_sol_v(var)
+    b.step(4)
+    b.checkpoint_write(tmp_path / "m.ckp")
+    c = Channel(pm, x3, jac, inv)
+    c.checkpoint_read(tmp_path / "m.ckp")
+    c.step(4)
+    assert np.array_equal(c.download(), ref)
+    assert a.debug_canaries() == 0 and c.debug_canaries() == 0
+
+
+@pytest.mark.parametrize("name", ["st4", "gst2", "s3", "rd1"])
+def test_mixed_wall_variants_track_fp64(name):
+    p, x3, jac, inv, var = make_case(nP=(24, 16, 21), mesh="tanh", beta=2.0, rk=RK3, Pr=0.72, istat=5,
+                                     quantize=False)
+    bottom, top = W.reference_variant(name, p)
+    g = Channel(p.with_(mixed=True), x3, jac, inv)
+    g.init_sol_v(var)
+    g.set_wall_bc(0, bottom); g.set_wall_bc(1, top)
+    o = O.Oracle(p, x3, jac, inv)
+    o.upload(var)
+    o.set_wall_bc(0, bottom); o.set_wall_bc(1, top)
+    g.step(20)
+    o.step(20)
+    assert np.all(rel_l2(g.download(), o.download()) <= MIXED_TOL)
