@@ -37,9 +37,9 @@ ISTAT = 10
 
 
 def workload(nP=GRID):
-    from compchan3dmpi_b200 import baseline_params, mesh_tanh, laminar_noise, cfl_dt
+    from compchan3dmpi_b200 import production_params, mesh_tanh, laminar_noise, cfl_dt
     x3, jac, inv = mesh_tanh(nP[2], BETA)
-    p = baseline_params(nP, istat=ISTAT)
+    p = production_params(nP, istat=ISTAT)
     var = laminar_noise(p, x3, seed=1234)
     p = p.with_(dt=cfl_dt(var, p, jac, CFL))
     return p, x3, jac, inv, var

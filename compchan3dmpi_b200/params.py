@@ -68,7 +68,7 @@ def reference_params(nP=(64, 48, 65), **kw) -> ChanParams:
     return ChanParams(nP=tuple(nP), **kw)
 
 
-def baseline_params(nP=(256, 192, 193), **kw) -> ChanParams:
+def production_params(nP=(256, 192, 193), **kw) -> ChanParams:
     """Production workload physics: SSP-RK3, Pr = 0.72 (dt is set from CFL by the caller)."""
     base = dict(Pr=0.72, rk_scheme=RK3)
     base.update(kw)
