@@ -876,17 +876,44 @@ __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, 
 }
 
 // QT: storage type of the stage output the wall BC reads (the planes next to the wall)
+constexpr int kWallBX = 32, kWallBY = 8;
 template <typename QT>
-__global__ void k_wall(const KParams P)
+__global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
 {
     const QT *qo = static_cast<const QT *>(P.qout);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int wall = blockIdx.z;
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
+    const long long plane = P.plane, vol = P.vol;
+    // primitives of the two planes next to the wall on the block's (i,j) tile
+    // plus a 1-point halo, each computed once: [plane][r,u,v,w,p,mu][by][bx]
+    constexpr int HX = kWallBX + 2, HY = kWallBY + 2;
+    __shared__ double sp[2][6][HY][HX];
+    {
+        const int k2 = wall == 0 ? 2 : n3 - 1, k3 = wall == 0 ? 3 : n3 - 2;
+        const int i0 = blockIdx.x * blockDim.x - 1, j0 = blockIdx.y * blockDim.y - 1;
+        for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < 2 * HX * HY; e += blockDim.x * blockDim.y) {
+            const int pl = e / (HX * HY), r0 = e - pl * HX * HY, by = r0 / HX, bx = r0 - by * HX;
+            const int ii = i0 + bx, jj = j0 + by;
+            if (ii < 1 || ii > n1 || jj < 1 || jj > n2) continue;
+            const long long o = (long long)(pl == 0 ? k2 : k3) * plane + (long long)jj * P.px + ii;
+            const double q0 = qo[o], q1 = qo[vol + o], q2 = qo[2 * vol + o];
+            const double q3 = qo[3 * vol + o], q4 = qo[4 * vol + o];
+            const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
+            const double E = q4 / q0;
+            const double T = E - P.ggMh * ((u * u + v * v) + w * w);
+            sp[pl][0][by][bx] = q0;
+            sp[pl][1][by][bx] = u;
+            sp[pl][2][by][bx] = v;
+            sp[pl][3][by][bx] = w;
+            sp[pl][4][by][bx] = (q0 * T) / P.gM2;
+            sp[pl][5][by][bx] = pow07(T);
+        }
+    }
+    __syncthreads();
     if (i > n1 + 1 || j > n2 + 1) return;
     if (frozen(P.status, P.step)) return;
-    const long long plane = P.plane, vol = P.vol;
     double *W = P.wp + (size_t)wall * 8 * plane;
     const long long idx = (long long)j * P.px + i;
     const bool custom = P.wall_custom != 0;
@@ -905,17 +932,18 @@ __global__ void k_wall(const KParams P)
         const double *c1 = wall == 0 ? P.f1 : P.b1;
         const double *c2 = wall == 0 ? P.f2 : P.b2;
         // primitive + mu of one interior point, as calcPrim/calcBC produce them
+        // (staged above); kk selects the plane k2 or k3
         auto prim = [&](int ii, int jj, int kk, double &r, double &u, double &v, double &w, double &T,
                         double &p, double &mu) {
-            const long long o = (long long)kk * plane + (long long)jj * P.px + ii;
-            const double q0 = qo[o], q1 = qo[vol + o], q2 = qo[2 * vol + o];
-            const double q3 = qo[3 * vol + o], q4 = qo[4 * vol + o];
-            r = q0;
-            u = q1 / q0; v = q2 / q0; w = q3 / q0;
-            const double E = q4 / q0;
-            T = E - P.ggMh * ((u * u + v * v) + w * w);
-            p = (r * T) / P.gM2;
-            mu = pow07(T);
+            const int pl = kk == k2 ? 0 : 1;
+            const int bx = ii - (int)(blockIdx.x * blockDim.x) + 1, by = jj - (int)(blockIdx.y * blockDim.y) + 1;
+            r = sp[pl][0][by][bx];
+            u = sp[pl][1][by][bx];
+            v = sp[pl][2][by][bx];
+            w = sp[pl][3][by][bx];
+            p = sp[pl][4][by][bx];
+            mu = sp[pl][5][by][bx];
+            T = 0.0;
         };
         // wall-point terms c0*mu_w*u_w of the neighbours (zero for a no-slip wall)
         double t_ip = 0.0, t_im = 0.0, t_jp = 0.0, t_jm = 0.0;
@@ -1015,7 +1043,7 @@ __device__ __forceinline__ double warp_sum(double v)
 // pb = n3, n3+1: the wall-shear sum of the bottom, top wall) into
 // part[(pb*S + sub)*23 + c].  Pass 2 adds the S partial sums in a fixed
 // order: the result is deterministic.
-__global__ void __launch_bounds__(kStatThreads) k_stats_part(const KParams P, const double *q, int do_moments,
+__global__ void __launch_bounds__(kStatThreads, 3) k_stats_part(const KParams P, const double *q, int do_moments,
                                                              int do_tau, int S, double *part)
 {
     __shared__ double red[kStatThreads / 32][23];
@@ -1031,6 +1059,7 @@ __global__ void __launch_bounds__(kStatThreads) k_stats_part(const KParams P, co
 #pragma unroll
         for (int c = 0; c < 23; c++) acc[c] = 0.0;
         const int np = n1 * n2;
+#pragma unroll 2
         for (int p = sub * kStatThreads + tid; p < np; p += S * kStatThreads) {
             const int jj = p / n1, ii = p - jj * n1;
             double x[7];

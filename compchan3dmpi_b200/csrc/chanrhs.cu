@@ -385,12 +385,12 @@ double *noalloc_scratch(int dev)
     return g_noalloc_addr[dev];
 }
 
-// blocks per plane of the statistics pass: about 8 blocks per SM, at least
+// blocks per plane of the statistics pass: about 16 blocks per SM, at least
 // 4 point strides per block, at most kMaxSplit
 int stats_split(int sms, int n1, int n2, int n3)
 {
     const long long np = (long long)n1 * n2;
-    int ns = (int)((8LL * sms + (n3 + 2) - 1) / (n3 + 2));
+    int ns = (int)((16LL * sms + (n3 + 2) - 1) / (n3 + 2));
     const int cap = (int)std::max<long long>(1, np / (4LL * chan::kStatThreads));
     ns = std::min(std::min(ns, cap), kMaxSplit);
     return std::max(ns, 1);
