@@ -130,7 +130,8 @@ def measured_traffic(p, n_int):
     """Per-launch DRAM bytes of the stage kernel: the per-point figure of the
     committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum over
     one RK3 step of a 4.6 M-point case) scaled by this workload's points."""
-    f = os.path.join(ROOT, "profiles", "stage_kernel_256x192x97_full.md")
+    name = "stage_kernel_mixed_256x192x97_full.md" if getattr(p, "mixed", False) else "stage_kernel_256x192x97_full.md"
+    f = os.path.join(ROOT, "profiles", name)
     try:
         with open(f) as fh:
             for ln in fh:
@@ -329,7 +330,7 @@ def run_ours(args):
             bpp = (80 + 120 * (stages - 1)) / stages   # algorithmic bytes per updated point per stage launch
         achieved = n_int * bpp / (stage_ms_max / 1e3) / 1e9
         peak, peak_kind = hbm_peak()
-        traffic = None if p.mixed else measured_traffic(p, n_int)
+        traffic = measured_traffic(p, n_int)
         # stage + wall-BC kernels per stage, plus the two statistics passes on their cadence
         launches = K * 2 * stages + 2 * sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
         line = {
