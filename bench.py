@@ -10,7 +10,11 @@ statistics every 10 steps.  It starts from the seeded laminar +-10 % start.
 One "step" is one full RK3 time step (3 stages).  The metric counts
 interior points x stages per second, summed over all GPUs (replicas).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--mixed]
+
+--mixed measures the mixed-precision path (float stage states and fluxes,
+double accumulation) on the same workload and adds its error against the
+FP64 path.
 """
 from __future__ import annotations
 
