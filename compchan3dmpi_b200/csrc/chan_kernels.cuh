@@ -173,6 +173,16 @@ struct SlotT {
     const R *U, *V, *W, *T;
 };
 
+// pressure at box point b.  With FP64 rings PR is the ring's pressure slot;
+// with float rings there is no pressure slot, PR is the density slot and p is
+// rho*T/(gama*Ma^2) formed on the spot (one multiply against two shared loads).
+template <typename R>
+__device__ __forceinline__ R pres_at(const FluxC<R> &C, const SlotT<R> &s, const R *PR, int b)
+{
+    if constexpr (sizeof(R) == 4) return (PR[b] * s.T[b]) * C.inv_gM2;
+    else return PR[b];
+}
+
 template <int BX, typename R>
 __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
                                         const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4])
@@ -185,7 +195,7 @@ __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, co
     const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
     const R uz = (sp.U[b] - sm.U[b]) * czt;
     const R wz = (sp.W[b] - sm.W[b]) * czt;
-    const R mu = MU[b], pr = PR[b];
+    const R mu = MU[b], pr = pres_at(C, s, PR, b);
     const R mr = mu * C.invRe;
     const R div = (ux + vy) + wz;
     const R f2 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * ux;
@@ -209,7 +219,7 @@ __device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, co
     const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
     const R vz = (sp.V[b] - sm.V[b]) * czt;
     const R wz = (sp.W[b] - sm.W[b]) * czt;
-    const R mu = MU[b], pr = PR[b];
+    const R mu = MU[b], pr = pres_at(C, s, PR, b);
     const R mr = mu * C.invRe;
     const R div = (ux + vy) + wz;
     const R g2 = -(mr * (vx + uy));
@@ -238,7 +248,7 @@ __device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, c
     const R uz = (sp.U[b] - sm.U[b]) * czt;
     const R vz = (sp.V[b] - sm.V[b]) * czt;
     const R wz = (sp.W[b] - sm.W[b]) * czt;
-    const R mu = MU[b], pr = PR[b];
+    const R mu = MU[b], pr = pres_at(C, s, PR, b);
     const R u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
     const R mr = mu * C.invRe, kqm = C.kq * mu;
     const R div = (ux + vy) + wz;
@@ -364,8 +374,15 @@ template <int TI, int TJ, typename R>
 struct StageShape {
     static constexpr int BX = TI + 4, BY = TJ + 4, NB = BX * BY, NT = TI * TJ;
     static constexpr int NFX = TJ * (TI + 2), NGY = (TJ + 2) * TI;
-    static constexpr int words = 12 * NB + 4 * NB + 10 * NB + 4 * NFX + 4 * NGY;
-    static constexpr size_t bytes = sizeof(R) * (size_t)words;
+    // float rings keep mu only and form p from rho and T where it is used;
+    // FP64 rings keep (mu, p)
+    static constexpr bool p_ring = sizeof(R) == 8;
+    static constexpr int words = 12 * NB + (p_ring ? 4 : 2) * NB + 10 * NB + 4 * NFX + 4 * NGY;
+    // float rings leave room to stage the RK base of every thread's own point
+    // (double) by cp.async; the FP64 rings do not fit it beside two CTAs per SM
+    static constexpr bool prefetch_base = sizeof(R) == 4;
+    static constexpr size_t bytes =
+        sizeof(R) * (size_t)words + (prefetch_base ? sizeof(double) * 5 * (size_t)NT : 0);
 };
 
 #ifndef CHAN_MINB
@@ -407,6 +424,16 @@ __device__ __forceinline__ float mu_of<float>(double T) { return exp2f(0.7f * lo
 template <typename T>
 __device__ __forceinline__ double ldq(const T *p) { return (double)__ldg(p); }
 
+// 8-byte asynchronous global->shared copy (no register staging)
+__device__ __forceinline__ void cp_async8(double *dst, const double *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <int TI, int TJ, typename QI, typename QO, typename R>
 __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MINB) k_stage(const KParams P)
 {
@@ -416,10 +443,11 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     static_assert(2 * TJ <= 32 && 32 + 2 * TI <= NT, "halo-flux lane layout needs 2*TJ <= 32 and 32+2*TI <= TI*TJ");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *sPr = reinterpret_cast<R *>(smem_raw);   // [3][4][NB]
-    R *sMP = sPr + 12 * NB;                     // [2][2][NB]   mu, p
-    R *sQ = sMP + 4 * NB;                       // [2][5][NB]
+    R *sMP = sPr + 12 * NB;                     // [2][2][NB] mu, p  ([2][NB] mu with float rings)
+    R *sQ = sMP + (S::p_ring ? 4 : 2) * NB;     // [2][5][NB]
     R *sF = sQ + 10 * NB;                       // [4][TJ][TI+2]
     R *sG = sF + 4 * S::NFX;                    // [4][TJ+2][TI]
+    double *sQB = reinterpret_cast<double *>(smem_raw + sizeof(R) * S::words);   // [5][NT] (float rings only)
     __shared__ int s_frozen;
     const FluxC<R> &C = fluxc<R>(P);
     // the state pointers are read from the parameter space at each use: held
@@ -447,13 +475,15 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     // ring slots by role, rotated once per plane instead of indexed by plane:
     // prims (u,v,w,T) for t-1, t, t+1 at offsets oM, oZ, oP; Q and (mu,p) for
     // t, t+1 at qZ, qP and mZ, mP (offsets in words)
-    int oM = 0, oZ = 4 * NB, oP = 8 * NB, qZ = 0, qP = 5 * NB, mZ = 0, mP = 2 * NB;
+    int oM = 0, oZ = 4 * NB, oP = 8 * NB, qZ = 0, qP = 5 * NB, mZ = 0, mP = (S::p_ring ? 2 : 1) * NB;
     auto slot = [&](int o) -> Slot {
         return Slot{sPr + o, sPr + o + NB, sPr + o + 2 * NB, sPr + o + 3 * NB};
     };
     auto smu = [&](int o) { return sMP + o; };
-    auto spr = [&](int o) { return sMP + o + NB; };
     auto sq = [&](int o, int v) { return sQ + o + v * NB; };
+    // what the flux helpers read the pressure from (pres_at): the p slot of
+    // the (mu,p) ring at mo, or the density of the Q ring at qo
+    auto spr = [&](int mo, int qo) { return S::p_ring ? sMP + mo + NB : sq(qo, 0); };
 
     // box points this thread loads: the same columns for every plane
     // lp: box index | 0x10000 if the point is in R1 (tile plus a 1-point cross
@@ -482,7 +512,7 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     // values from memory instead (hflux_wall).
     auto load_plane = [&](int m, int po, int qo, int mo) {
         const Slot s = slot(po);
-        R *MU = smu(mo), *PR = spr(mo);
+        R *MU = smu(mo), *PR = sMP + mo + NB;
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
 #pragma unroll
@@ -517,7 +547,7 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
             ((R *)s.W)[p] = (R)w;
             ((R *)s.T)[p] = (R)T;
             MU[p] = mu;
-            PR[p] = (R)pr;
+            if (S::p_ring) PR[p] = (R)pr;
         }
     };
 
@@ -535,10 +565,10 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     };
 
     // hD at the own column of interior plane m (in ring); dz from (m-1, m+1) values
-    auto hflux = [&](int m, int po, int mo, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
+    auto hflux = [&](int m, int po, int mo, int qo, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
         const Slot s = slot(po);
         const R sc = ktab<R>(P, 0, m);
-        visc_fz<BX>(C, s, smu(mo)[bc], spr(mo)[bc], bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
+        visc_fz<BX>(C, s, smu(mo)[bc], pres_at(C, s, spr(mo, qo), bc), bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
                     (Tp - Tm) * sc, h);
     };
     // hD at the own column of wall plane m, from the wall's own values in
@@ -577,13 +607,13 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
             } else {
                 double q[5], u, v, w, T;
                 center(kb - 2, q, u, v, w, T);
-                hflux(kb - 1, oM, mP, (R)u, (R)v, (R)w, (R)T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                hflux(kb - 1, oM, mP, qP, (R)u, (R)v, (R)w, (R)T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
             }
             // hD(kb)
             {
                 double q[5], u, v, w, T;
                 center(kb + 1, q, u, v, w, T);
-                hflux(kb, oZ, mZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], (R)u, (R)v, (R)w, (R)T, h0);
+                hflux(kb, oZ, mZ, qZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], (R)u, (R)v, (R)w, (R)T, h0);
             }
             if (kb - 2 >= 1) {
                 double q[5], u, v, w, T;
@@ -610,7 +640,16 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     __syncthreads();
 
     for (int t = kb; t <= ke; t++) {
-        // ---------- A: plane t+1 into the ring; own column of t+2
+        // ---------- A: plane t+1 into the ring; own column of t+2 (and, with
+        // float rings, the own point's RK base starts its way into shared memory)
+        if (S::prefetch_base) {
+            if (P.rk_mode != 0 && out_ok) {
+                const double *src = P.qbase + (long long)t * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) cp_async8(sQB + c * NT + tid, src + c * vol);
+            }
+            cp_async_commit();
+        }
         load_plane(t + 1, oP, qP, mP);
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
         if (col_ok && t + 2 <= n3) {
@@ -627,10 +666,10 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
         R hp1[4] = {0, 0, 0, 0};
         {
             const R czt = ktab<R>(P, 0, t);
-            const R *MU = smu(mZ), *PR = spr(mZ);
+            const R *MU = smu(mZ), *PR = spr(mZ, qZ);
             if (col_ok) {
                 if (t + 1 != n3)
-                    hflux(t + 1, oP, mP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+                    hflux(t + 1, oP, mP, qP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 R f[4], g[4];
                 visc_fxy<BX>(C, s0, sm, sp, MU, PR, bc, czt, f, g);
 #pragma unroll
@@ -760,9 +799,15 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
             double qn[5];
             double qb[5] = {0, 0, 0, 0, 0};
             if (P.rk_mode != 0) {
-                const long long off = (long long)t * plane + colo;
+                if (S::prefetch_base) {
+                    cp_async_wait<0>();
 #pragma unroll
-                for (int c = 0; c < 5; c++) qb[c] = __ldg(P.qbase + c * vol + off);
+                    for (int c = 0; c < 5; c++) qb[c] = sQB[c * NT + tid];
+                } else {
+                    const long long off = (long long)t * plane + colo;
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qb[c] = __ldg(P.qbase + c * vol + off);
+                }
             }
             if (P.rk_mode == 0) {
 #pragma unroll
@@ -816,6 +861,7 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
         }
         __syncthreads();
     }
+    if (S::prefetch_base) cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
