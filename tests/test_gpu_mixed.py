@@ -86,3 +86,24 @@ def test_mixed_wall_variants_track_fp64(name):
     g.step(20)
     o.step(20)
     assert np.all(rel_l2(g.download(), o.download()) <= MIXED_TOL)
+
+
+def test_mixed_check_long_run_profiles_small_grid():
+    """mixed_check.compare on a small grid: the averaged profiles in wall units
+    (Cf, u+, rms, <u'w'>) of the mixed path stay close to the FP64 path's."""
+    from compchan3dmpi_b200 import mixed_check
+    p, x3, jac, inv, var = make_case(nP=(32, 24, 33), mesh="tanh", beta=2.2, rk=RK3, Pr=0.72, istat=10, cfl=0.6)
+    # this coarse grid stays stable for about 240 steps
+    r = mixed_check.compare(p, x3, jac, inv, var, steps=200, avg_from=100, every=50)
+    assert [s["step"] for s in r["series"]] == [50, 100, 150, 200]
+    for s in r["series"]:
+        assert np.all(np.array(s["rel_l2"]) <= MIXED_TOL), s
+    pr = r["profiles"]
+    assert pr["samples"] == 10
+    assert pr["Cf"]["fp64"] > 0 and pr["Cf"]["rel_err"] <= 1e-4
+    assert pr["uplus_rel_err"] <= 1e-4
+    for v in ("rho", "u", "E", "T", "p"):
+        assert pr["mean_rel_err"][v] <= 1e-4, v
+    assert pr["rms_rel_err"]["u"] <= 1e-3
+    assert pr["uw_rel_err"] <= 1e-3
+    assert r["wall_s"]["fp64"] > 0 and r["wall_s"]["mixed"] > 0

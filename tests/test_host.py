@@ -198,3 +198,11 @@ def test_driver_event_cadence_and_debug_format(tmp_path):
     assert lines[0] == 'TITLE ="        0.2500000000        7"'
     assert lines[5] == "  0.0000  0.0000  0.0000  0.15000E+01  0.00000E+00  0.00000E+00  0.00000E+00" \
                        "  0.00000E+00 -0.25000E-02  0.00000E+00"
+
+
+def test_mixed_check_rejects_bad_windows_before_any_device_work():
+    from compchan3dmpi_b200 import mixed_check, production_params
+    p = production_params((20, 14, 19), istat=10)
+    for steps, avg_from, every in ((1000, 500, 300), (1000, 1000, 100), (1000, 200, 15), (950, 100, 100)):
+        with pytest.raises(ValueError):
+            mixed_check.compare(p, None, None, None, None, steps, avg_from, every)
