@@ -15,6 +15,10 @@ interior points x stages per second, summed over all GPUs (replicas).
 --mixed measures the mixed-precision path (float stage states and fluxes,
 double accumulation) on the same workload and adds its error against the
 FP64 path.
+
+--ensemble measures the stratified parameter sweep (16 mixed-precision cases
+of uneven grids) stepped as one graph-replayed ensemble with autotuned launch
+shapes, next to the same cases run one at a time.
 """
 from __future__ import annotations
 
@@ -363,6 +367,122 @@ def run_ours(args):
     return 0
 
 
+def run_ensemble(args):
+    """--ensemble: the stratified parameter sweep (compchan3dmpi_b200.ensemble:
+    16 mixed-precision cases of uneven grids, per-case Ma, Re, Ri, dT) as one
+    ensemble -- graph replays of all members concurrently, launch shapes from
+    the autotuner -- against the same cases run one at a time."""
+    import torch
+    from compchan3dmpi_b200 import replicas as R
+    from compchan3dmpi_b200.ensemble import Ensemble, open_case, sweep_cases
+
+    ranks = R.init("nccl" if args.gpus > 1 else "gloo")
+    dev = ranks.local_rank
+    torch.cuda.set_device(dev)
+    cases = sweep_cases(args.members)
+    for c in cases:
+        c.params = c.params.with_(device=dev)
+    L = ISTAT
+    K = max(L, (args.steps + L - 1) // L * L)   # whole graph blocks
+    W = max(args.warmup, 3)
+    per_step = sum(c.params.n_interior * c.params.stages for c in cases)
+
+    # one at a time: each case alone with its default launch shape
+    solo_ms = 0.0
+    for c in cases:
+        ch = open_case(c)
+        ch.step(W)
+        stream = torch.cuda.ExternalStream(ch.stream_handle(), device=torch.device("cuda", dev))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ch.sync()
+        ev0.record(stream)
+        ch.step_async(K)
+        ev1.record(stream)
+        ch.sync()
+        torch.cuda.synchronize()
+        solo_ms += ev0.elapsed_time(ev1)
+        ch.close()
+
+    chans = [open_case(c) for c in cases]
+    e = Ensemble(chans)
+    clocks = Clocks(dev)
+    e.step(W)
+    R.barrier(ranks)
+    clocks.start()
+    st0 = e.step(K)
+    untuned_ms = e.last_replay_ms()
+    tune_ms = e.tune(reps=3)
+    e.step(W)
+    st1 = e.step(K)
+    tuned_ms = e.last_replay_ms()
+    ck = clocks.stop()
+    shapes = e.launch_shapes()
+    replays, captures = e.counters()
+
+    # end to end: upload every member from pinned host memory, K steps, download every member
+    host_in = [torch.empty(c.var.shape, dtype=torch.float64).pin_memory() for c in cases]
+    host_out = [torch.empty(c.var.shape, dtype=torch.float64).pin_memory() for c in cases]
+    for h, c in zip(host_in, cases):
+        h.numpy()[...] = c.var
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for ch, h in zip(chans, host_in):
+        ch.init_sol_v(h.numpy())
+    st2 = e.step(K)
+    for ch, h in zip(chans, host_out):
+        ch.download(out=h.numpy())
+    e2e_s = time.perf_counter() - t0
+    e.close()
+    for ch in chans:
+        ch.close()
+    R.barrier(ranks)
+    tuned_max = R.max_over_ranks(ranks, tuned_ms)
+    solo_max = R.max_over_ranks(ranks, solo_ms)
+    e2e_max = R.max_over_ranks(ranks, e2e_s)
+    if ranks.is_root:
+        value = ranks.world * per_step * K / (tuned_max / 1e3)
+        solo = ranks.world * per_step * K / (solo_max / 1e3)
+        bpp = 240.0 / 3.0   # mixed RK3: algorithmic bytes per updated point per stage
+        achieved = per_step * bpp * K / (tuned_max / 1e3) / 1e9
+        peak, peak_kind = hbm_peak()
+        n_pts = sum(int(np.prod(c.params.nP)) for c in cases)
+        launches = K * sum(1 + 2 * c.params.stages for c in cases) + (K // L) * 2 * len(cases)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
+            "ms_per_step": tuned_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (seeded stratified laminar starts, +-10% noise)",
+            "config": {
+                "workload": f"stratified sweep ensemble: {len(cases)} mixed-precision SSP-RK3 cases, "
+                            f"grids nP (64,64,65)..(160,128,129), CFL 0.6, tanh beta 2.2",
+                "members": [{"nP": list(c.params.nP), "Ma": c.params.Mac, "Re": c.params.Re, "Ri": c.Ri,
+                             "dT": c.dT} for c in cases],
+                "updated_points": per_step // 3, "istat": ISTAT, "graph_block_steps": L,
+                "parallelism": f"replicas x{ranks.world}",
+                "l2_policy": "members' states together larger than L2 (126 MB); no flush"},
+            "one_at_a_time": {"value": solo, "ms_per_step": solo_max / K,
+                              "how": "each case alone, default launch shape, CUDA events on its stream"},
+            "speedup_vs_one_at_a_time": value / solo,
+            "untuned": {"value": per_step * K / (untuned_ms / 1e3), "ms_per_step": untuned_ms / K},
+            "autotuner": {"trial_ms": tune_ms, "shapes": [list(x) for x in shapes]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "every member's k_stage (whole ensemble step)",
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "e2e": {"value": ranks.world * per_step * K / e2e_max, "unit": UNIT,
+                    "h2d_bytes_per_step": 7 * 8 * n_pts / K, "d2h_bytes_per_step": 7 * 8 * n_pts / K,
+                    "calls": "chan_upload of every member + chan_ensemble_step(K) + chan_download of every "
+                             "member (host wall clock around the synchronous calls)"},
+            "gpu_launches": int(launches),
+            "graph": {"replays": replays, "captures": captures},
+            "clocks": ck,
+            "status_ok": all(x == 0 for x in st0 + st1 + st2),
+        }
+        print(json.dumps(line), flush=True)
+    R.finalize(ranks)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,11 +494,16 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--mixed", action="store_true",
                     help="mixed precision: float stage storage and fluxes, double accumulation")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="the stratified parameter sweep as one graph-replayed ensemble vs one case at a time")
+    ap.add_argument("--members", type=int, default=16, help="ensemble size for --ensemble")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.ensemble:
+        return run_ensemble(args)
     return run_ours(args)
 
 

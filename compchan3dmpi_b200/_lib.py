@@ -100,7 +100,23 @@ SIGNATURES = [
     ("chan_io_last_error", ctypes.c_char_p, []),
     ("chan_avg_spatial_noalloc", ctypes.c_int, [_D, _I32, _D, _D, _D, ctypes.c_int32]),
     ("chan_free", None, [ctypes.c_void_p]),
+    ("chan_set_buoyancy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
+    ("chan_set_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    ("chan_get_launch", ctypes.c_int, [ctypes.c_void_p, _I32, _I32, _I32]),
+    ("chan_ensemble_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    ("chan_ensemble_size", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_ensemble_block", ctypes.c_int, [ctypes.c_void_p]),
+    ("chan_ensemble_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _I32]),
+    ("chan_ensemble_tune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _D]),
+    ("chan_ensemble_counters", ctypes.c_int, [ctypes.c_void_p, _I64, _I64, _D]),
+    ("chan_ensemble_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("chan_ensemble_free", None, [ctypes.c_void_p]),
 ]
+
+CHAN_TILE_32x8 = 0
+CHAN_TILE_32x4 = 1
+CHAN_NTILES = 2
 
 _lib = None
 

@@ -85,6 +85,9 @@ class Channel:
         raise ChanError(r, self.L.chan_last_error(self._h).decode())
 
     def close(self):
+        ens = getattr(self, "_ensemble", None)
+        if ens is not None:   # an ensemble is freed before its members
+            ens.close()
         if getattr(self, "_h", None):
             self.L.chan_free(self._h)
             self._h = None
@@ -229,6 +232,21 @@ class Channel:
                                               None if fl is None else _lib.dptr(fl),
                                               None if q is None else _lib.dptr(q)))
         return fl, q
+
+    def set_buoyancy(self, Ri: float, Tref: float = 1.0):
+        """Buoyancy body force Ri*rho*(T - Tref) on the wall-normal momentum
+        (and its work on the energy); Ri = 0 switches it off."""
+        self._check(self.L.chan_set_buoyancy(self._h, float(Ri), float(Tref)))
+
+    def set_launch(self, tile: int = 0, nchunks: int = 0):
+        """Stage-kernel launch shape: tile 0 (32x8) or 1 (32x4), k-chunks (0: automatic)."""
+        self._check(self.L.chan_set_launch(self._h, int(tile), int(nchunks)))
+
+    def launch(self):
+        """(tile, nchunks, planes per chunk) of the stage kernel."""
+        t, n, k = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self.L.chan_get_launch(self._h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(k)))
+        return t.value, n.value, k.value
 
     def set_forcing(self, tauL: float, tauU: float, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)

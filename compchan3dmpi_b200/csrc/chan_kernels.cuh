@@ -24,6 +24,14 @@
 
 namespace chan {
 
+// Step counter and time of the step being computed, kept on the device for
+// launches replayed from a CUDA graph (whose kernel arguments are fixed at
+// capture); k_clock_advance moves it at the start of every step.
+struct DevClock {
+    long long step;
+    double time;
+};
+
 struct DevStatus {
     int blown;             // rho<0 or T<0 seen (reference blow-up test)
     int ijk[3];            // one offending point, 1-based reference indices
@@ -98,9 +106,19 @@ struct KParams {
     int acc_on;           // statistics steps also add into tacc (time averaging)
     int wall_custom;      // any wall uses a non-default WallBC
     WallBC wbc[2];
+    // buoyancy body force ri*rho*(T - tref) on the wall-normal momentum and its
+    // work ggM*w*(that) on the energy (a Boussinesq-style term for stratified
+    // sweeps; the reference has none).  buoy_on = 0 leaves the RHS unchanged.
+    double ri, tref;
+    int buoy_on;
     double time;          // time of the step being computed (the reference's `time`)
     long long step;       // step number being computed
+    const DevClock *clk;  // non-null in graph replays: step and time come from here
 };
+
+// step / time of the step being computed (kernel argument, or the device clock)
+__device__ __forceinline__ long long kstep(const KParams &P) { return P.clk ? P.clk->step : P.step; }
+__device__ __forceinline__ double ktime(const KParams &P) { return P.clk ? P.clk->time : P.time; }
 
 __device__ __forceinline__ bool frozen(const DevStatus *st, long long step)
 {
@@ -183,6 +201,59 @@ __device__ __forceinline__ R pres_at(const FluxC<R> &C, const SlotT<R> &s, const
     else return PR[b];
 }
 
+// Single-rounding multiply-add in the ring type.  The viscous fluxes are
+// written with explicit FMAs so that every place that evaluates one (own
+// columns, halo lanes, the k-march prologue) rounds it the same way, and a
+// point's result does not depend on the launch shape that computed it.
+template <typename R>
+__device__ __forceinline__ R fmaR(R a, R b, R c);
+template <>
+__device__ __forceinline__ double fmaR<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <>
+__device__ __forceinline__ float fmaR<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// an add the compiler may not fuse with a product feeding it
+template <typename R>
+__device__ __forceinline__ R addR(R a, R b);
+template <>
+__device__ __forceinline__ double addR<double>(double a, double b) { return __dadd_rn(a, b); }
+template <>
+__device__ __forceinline__ float addR<float>(float a, float b) { return __fadd_rn(a, b); }
+
+// fD from the gradients at one point: [p + 2/3 mu/Re div - 2 mu/Re u_x,
+// -mu/Re (v_x+u_y), -mu/Re (w_x+u_z), -kq mu T_x + ggM (u fD2 + v fD3 + w fD4)]
+template <typename R>
+__device__ __forceinline__ void fd_point(const FluxC<R> &C, R mu, R pr, R u0, R v0, R w0, R ux, R vy, R wz, R vx,
+                                         R uy, R wx, R uz, R Tx, R f[4])
+{
+    const R mr = mu * C.invRe, kqm = C.kq * mu;
+    const R div = addR(addR(ux, vy), wz);
+    const R pd = fmaR(C.two3rd * mr, div, pr);
+    const R t12 = mr * addR(vx, uy);
+    const R f2 = fmaR(-(R(2) * mr), ux, pd);
+    const R f4 = -(mr * addR(wx, uz));
+    f[0] = f2;
+    f[1] = -t12;
+    f[2] = f4;
+    f[3] = fmaR(C.ggM, fmaR(w0, f4, fmaR(u0, f2, -(v0 * t12))), -(kqm * Tx));
+}
+
+// gD from the gradients at one point (gD2 = fD3, the shared shear stress)
+template <typename R>
+__device__ __forceinline__ void gd_point(const FluxC<R> &C, R mu, R pr, R u0, R v0, R w0, R ux, R vy, R wz, R vx,
+                                         R uy, R wy, R vz, R Ty, R g[4])
+{
+    const R mr = mu * C.invRe, kqm = C.kq * mu;
+    const R div = addR(addR(ux, vy), wz);
+    const R pd = fmaR(C.two3rd * mr, div, pr);
+    const R t12 = mr * addR(vx, uy);
+    const R g3 = fmaR(-(R(2) * mr), vy, pd);
+    const R g4 = -(mr * addR(wy, vz));
+    g[0] = -t12;
+    g[1] = g3;
+    g[2] = g4;
+    g[3] = fmaR(C.ggM, fmaR(w0, g4, fmaR(v0, g3, -(u0 * t12))), -(kqm * Ty));
+}
+
 template <int BX, typename R>
 __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
                                         const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4])
@@ -195,16 +266,7 @@ __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, co
     const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
     const R uz = (sp.U[b] - sm.U[b]) * czt;
     const R wz = (sp.W[b] - sm.W[b]) * czt;
-    const R mu = MU[b], pr = pres_at(C, s, PR, b);
-    const R mr = mu * C.invRe;
-    const R div = (ux + vy) + wz;
-    const R f2 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * ux;
-    const R f3 = -(mr * (vx + uy));
-    const R f4 = -(mr * (wx + uz));
-    f[0] = f2;
-    f[1] = f3;
-    f[2] = f4;
-    f[3] = -((C.kq * mu) * Tx) + C.ggM * ((s.U[b] * f2 + s.V[b] * f3) + s.W[b] * f4);
+    fd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wx, uz, Tx, f);
 }
 
 template <int BX, typename R>
@@ -219,16 +281,7 @@ __device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, co
     const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
     const R vz = (sp.V[b] - sm.V[b]) * czt;
     const R wz = (sp.W[b] - sm.W[b]) * czt;
-    const R mu = MU[b], pr = pres_at(C, s, PR, b);
-    const R mr = mu * C.invRe;
-    const R div = (ux + vy) + wz;
-    const R g2 = -(mr * (vx + uy));
-    const R g3 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * vy;
-    const R g4 = -(mr * (wy + vz));
-    g[0] = g2;
-    g[1] = g3;
-    g[2] = g4;
-    g[3] = -((C.kq * mu) * Ty) + C.ggM * ((s.U[b] * g2 + s.V[b] * g3) + s.W[b] * g4);
+    gd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wy, vz, Ty, g);
 }
 
 // fD and gD together at one point: they share eight gradients, the shear
@@ -250,38 +303,23 @@ __device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, c
     const R wz = (sp.W[b] - sm.W[b]) * czt;
     const R mu = MU[b], pr = pres_at(C, s, PR, b);
     const R u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
-    const R mr = mu * C.invRe, kqm = C.kq * mu;
-    const R div = (ux + vy) + wz;
-    const R pd = pr + (C.two3rd * mr) * div;
-    const R t12 = mr * (vx + uy);
-    const R f2 = pd - (R(2) * mr) * ux;
-    const R f4 = -(mr * (wx + uz));
-    const R g3 = pd - (R(2) * mr) * vy;
-    const R g4 = -(mr * (wy + vz));
-    f[0] = f2;
-    f[1] = -t12;
-    f[2] = f4;
-    f[3] = -(kqm * Tx) + C.ggM * ((u0 * f2 - v0 * t12) + w0 * f4);
-    g[0] = -t12;
-    g[1] = g3;
-    g[2] = g4;
-    g[3] = -(kqm * Ty) + C.ggM * ((-(u0 * t12) + v0 * g3) + w0 * g4);
+    fd_point(C, mu, pr, u0, v0, w0, ux, vy, wz, vx, uy, wx, uz, Tx, f);
+    gd_point(C, mu, pr, u0, v0, w0, ux, vy, wz, vx, uy, wy, vz, Ty, g);
 }
 
-// hD from its in-plane derivatives, point values and z-derivatives
 template <typename R>
 __device__ __forceinline__ void visc_fz_vals(const FluxC<R> &C, R ux, R vy, R wx, R wy, R u, R v, R w, R mu, R pr,
                                              R uz, R vz, R wz, R Tz, R h[4])
 {
-    const R mr = mu * C.invRe;
-    const R div = (ux + vy) + wz;
-    const R h2 = -(mr * (wx + uz));
-    const R h3 = -(mr * (wy + vz));
-    const R h4 = (pr + (C.two3rd * mr) * div) - (R(2) * mr) * wz;
+    const R mr = mu * C.invRe, kqm = C.kq * mu;
+    const R div = addR(addR(ux, vy), wz);
+    const R h2 = -(mr * addR(wx, uz));
+    const R h3 = -(mr * addR(wy, vz));
+    const R h4 = fmaR(-(R(2) * mr), wz, fmaR(C.two3rd * mr, div, pr));
     h[0] = h2;
     h[1] = h3;
     h[2] = h4;
-    h[3] = -((C.kq * mu) * Tz) + C.ggM * ((u * h2 + v * h3) + w * h4);
+    h[3] = fmaR(C.ggM, fmaR(w, h4, fmaR(v, h3, u * h2)), -(kqm * Tz));
 }
 
 // hD at the thread's own column; z-derivatives supplied by the caller
@@ -347,7 +385,8 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
     v = q[2] * r;
     w = q[3] * r;
     const double E = q[4] * r;
-    T = E - P.ggMh * ((u * u + v * v) + w * w);
+    // explicit FMAs: the same bits wherever a point's primitives are formed
+    T = __fma_rn(-P.ggMh, __fma_rn(w, w, __fma_rn(v, v, u * u)), E);
 }
 
 // ---------------------------------------------------------------------------
@@ -370,6 +409,13 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
 // intermediate stage states in float and evaluates the fluxes in float; the
 // primitive recovery (T from the total energy), the RK update against the
 // double base state, the forcing and the blow-up test stay in double.
+#ifndef CHAN_MINB
+#define CHAN_MINB 2   // resident 256-thread CTAs per SM the register budget is sized for (FP64 rings)
+#endif
+#ifndef CHAN_MINB_F
+#define CHAN_MINB_F 3 // the same with float rings (half the shared memory)
+#endif
+
 template <int TI, int TJ, typename R>
 struct StageShape {
     static constexpr int BX = TI + 4, BY = TJ + 4, NB = BX * BY, NT = TI * TJ;
@@ -383,14 +429,15 @@ struct StageShape {
     static constexpr bool prefetch_base = sizeof(R) == 4;
     static constexpr size_t bytes =
         sizeof(R) * (size_t)words + (prefetch_base ? sizeof(double) * 5 * (size_t)NT : 0);
+    // resident CTAs per SM the register budget is sized for: 128 (FP64) or 80
+    // (float) registers per thread at 256 threads, but never more CTAs than
+    // the 228 KB of shared memory per SM holds (1 KB of it reserved per CTA)
+    static constexpr int minb_regs = (sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MINB) * 256 / NT;
+    static constexpr int minb_smem = (int)(233472 / (bytes + 1024));
+    static constexpr int minb = minb_regs < minb_smem ? minb_regs : minb_smem;
 };
 
-#ifndef CHAN_MINB
-#define CHAN_MINB 2   // resident CTAs per SM the register budget is sized for (FP64 rings)
-#endif
-#ifndef CHAN_MINB_F
-#define CHAN_MINB_F 3 // the same with float rings (half the shared memory)
-#endif
+
 
 template <typename R>
 __device__ __forceinline__ const FluxC<R> &fluxc(const KParams &P);
@@ -434,8 +481,8 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int TI, int TJ, typename QI, typename QO, typename R>
-__global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MINB) k_stage(const KParams P)
+template <int TI, int TJ, typename QI, typename QO, typename R, bool BUOY>
+__global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(const KParams P)
 {
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
@@ -456,7 +503,7 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
     auto qout = [&]() { return static_cast<QO *>(P.qout); };
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
-    if (tid == 0) s_frozen = frozen(P.status, P.step) ? 1 : 0;
+    if (tid == 0) s_frozen = frozen(P.status, kstep(P)) ? 1 : 0;
     __syncthreads();
     if (s_frozen) return;
 
@@ -785,6 +832,12 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
             Rd[1] = src2 - (double)Fs[1];
             Rd[2] = -(double)Fs[2];
             Rd[3] = -(double)Fs[3];
+            if (BUOY) {
+                // buoyancy on the wall-normal momentum and its work on the energy
+                const double bq = P.ri * ((double)q0[0] * ((double)s0.T[bc] - P.tref));
+                Rd[3] = bq - (double)Fs[3];
+                src5 = src5 + (P.ggM * (double)s0.W[bc]) * bq;
+            }
             Rd[4] = src5 - (double)Fs[4];
             // RK update in double, on the stage input at its stored precision
             double qs[5];
@@ -834,7 +887,7 @@ __global__ void __launch_bounds__(TI *TJ, sizeof(R) == 4 ? CHAN_MINB_F : CHAN_MI
             }
             if (P.check) {
                 const double tr = qn[0] * qn[4] - P.ggMh * ((qn[1] * qn[1] + qn[2] * qn[2]) + qn[3] * qn[3]);
-                if (qn[0] < 0.0 || (qn[0] > 0.0 && tr < 0.0)) flag_blown(P.status, i, j, t, P.step);
+                if (qn[0] < 0.0 || (qn[0] > 0.0 && tr < 0.0)) flag_blown(P.status, i, j, t, kstep(P));
                 bool fin = true;
 #pragma unroll
                 for (int c = 0; c < 5; c++) fin = fin && isfinite(qn[c]);
@@ -916,7 +969,7 @@ __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, 
         v = B.uv[n1 * n2 + (jc - 1) * n1 + ic - 1];
     } else if (B.vel == 3) {
         const double x = B.x1[ic - 1];
-        v = B.A * sin((B.kx * x + B.om * P.time) + ((jc & 1) ? B.ph : 0.0));
+        v = B.A * sin((B.kx * x + B.om * ktime(P)) + ((jc & 1) ? B.ph : 0.0));
     }
     T = (B.therm == 1) ? ((B.dTdz - c[1] * T2) - c[2] * T3) / c[0] : B.Tw;
 }
@@ -959,7 +1012,7 @@ __global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
     }
     __syncthreads();
     if (i > n1 + 1 || j > n2 + 1) return;
-    if (frozen(P.status, P.step)) return;
+    if (frozen(P.status, kstep(P))) return;
     double *W = P.wp + (size_t)wall * 8 * plane;
     const long long idx = (long long)j * P.px + i;
     const bool custom = P.wall_custom != 0;
@@ -1037,7 +1090,7 @@ __global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
     W[6 * plane + idx] = pnew;
     W[7 * plane + idx] = muw;
     if (P.check && i >= 1 && i <= n1 && j >= 1 && j <= n2) {
-        if (rho < 0.0 || Tw < 0.0) flag_blown(P.status, i, j, wall == 0 ? 1 : n3, P.step);
+        if (rho < 0.0 || Tw < 0.0) flag_blown(P.status, i, j, wall == 0 ? 1 : n3, kstep(P));
         if (!isfinite(rho) || !isfinite(pnew)) flag_nonfinite(P.status, i, j, wall == 0 ? 1 : n3);
     }
 }
@@ -1096,7 +1149,7 @@ __global__ void __launch_bounds__(kStatThreads, 3) k_stats_part(const KParams P,
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
     const int pb = blockIdx.x / S, sub = blockIdx.x - pb * S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (frozen(P.status, P.step + 1)) return;
+    if (frozen(P.status, kstep(P) + 1)) return;
     double *out = part + ((size_t)pb * S + sub) * 23;
     if (pb < n3) {
         if (!do_moments) return;
@@ -1173,7 +1226,7 @@ __global__ void k_stats_fin(const KParams P, int do_moments, int do_tau, int S, 
 {
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
     const int pb = blockIdx.x, c = threadIdx.x;
-    if (frozen(P.status, P.step + 1)) return;
+    if (frozen(P.status, kstep(P) + 1)) return;
     const double *in = part + (size_t)pb * S * 23;
     if (pb < n3) {
         if (!do_moments || c >= 23) return;
@@ -1223,7 +1276,7 @@ __global__ void __launch_bounds__(kStatThreads) k_diag_ke(const KParams P, const
     __shared__ double red[kStatThreads / 32];
     const int n1 = P.n1, n2 = P.n2;
     const int k = blockIdx.x + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (frozen(P.status, P.step + 1)) return;
+    if (frozen(P.status, kstep(P) + 1)) return;
     double acc = 0.0;
     const int np = n1 * n2;
     for (int p = tid; p < np; p += kStatThreads) {
@@ -1249,7 +1302,7 @@ __global__ void __launch_bounds__(kStatThreads) k_diag_fin(const KParams P, cons
     __shared__ double red[kStatThreads / 32];
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
     const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (frozen(P.status, P.step + 1)) {
+    if (frozen(P.status, kstep(P) + 1)) {
         if (b == 0 && tid == 0) rec[0] = -1.0;
         return;
     }
@@ -1257,7 +1310,7 @@ __global__ void __launch_bounds__(kStatThreads) k_diag_fin(const KParams P, cons
         if (tid == 0) {
             double t = 0.0;
             for (int k = 0; k < n3; k++) t += D.part[k];
-            rec[0] = (double)P.step;
+            rec[0] = (double)kstep(P);
             rec[1] = time;
             rec[2] = t / ((double)n1 * (double)n2 * (double)n3);
         }
@@ -1455,7 +1508,16 @@ __global__ void k_check(const KParams P, const double *q)
         const int kk = (int)(p / ((long long)n1 * n2));
         double x[7];
         ref_var(P, q, ii + 1, jj + 1, kk + 1, x);
-        if (x[0] < 0.0 || x[5] < 0.0) flag_blown(P.status, ii + 1, jj + 1, kk + 1, P.step);
+        if (x[0] < 0.0 || x[5] < 0.0) flag_blown(P.status, ii + 1, jj + 1, kk + 1, kstep(P));
+    }
+}
+
+// start of a step in a graph replay: step += 1, time += dt (the host's order)
+__global__ void k_clock_advance(DevClock *clk, double dt)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        clk->step = clk->step + 1;
+        clk->time = clk->time + dt;
     }
 }
 

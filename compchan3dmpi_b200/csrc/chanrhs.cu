@@ -16,15 +16,37 @@
 
 namespace {
 
-// stage-kernel tile: TI columns in x (one warp row) by TJ rows in y
-#ifndef CHAN_TI
-#define CHAN_TI 32
-#endif
-#ifndef CHAN_TJ
-#define CHAN_TJ 8
-#endif
-constexpr int TI = CHAN_TI;
-constexpr int TJ = CHAN_TJ;
+// Stage-kernel tile shapes: TI columns in x (one warp row) by TJ rows in y.
+// Each shape has the plain FP64 kernel and the three mixed-precision stage
+// kernels, without and with the buoyancy term.
+using StageFn = void (*)(const chan::KParams);
+struct StageSet {
+    int ti, tj;
+    StageFn k[2][4];   // [buoyancy][0 FP64, 1 mixed first stage, 2 mixed middle, 3 mixed last]
+    size_t smem, smemf;
+};
+template <int TI_, int TJ_, bool B>
+void fill_stage_set(StageSet &s)
+{
+    s.k[B][0] = chan::k_stage<TI_, TJ_, double, double, double, B>;
+    s.k[B][1] = chan::k_stage<TI_, TJ_, double, float, float, B>;
+    s.k[B][2] = chan::k_stage<TI_, TJ_, float, float, float, B>;
+    s.k[B][3] = chan::k_stage<TI_, TJ_, float, double, float, B>;
+}
+template <int TI_, int TJ_>
+StageSet make_stage_set()
+{
+    StageSet s{};
+    s.ti = TI_;
+    s.tj = TJ_;
+    fill_stage_set<TI_, TJ_, false>(s);
+    fill_stage_set<TI_, TJ_, true>(s);
+    s.smem = chan::StageShape<TI_, TJ_, double>::bytes;
+    s.smemf = chan::StageShape<TI_, TJ_, float>::bytes;
+    return s;
+}
+// CHAN_TILE_32x8 (default) and CHAN_TILE_32x4
+const StageSet kStageSets[CHAN_NTILES] = {make_stage_set<32, 8>(), make_stage_set<32, 4>()};
 constexpr int kMaxSplit = 16;   // statistics blocks per plane, at most
 
 std::string g_init_error;
@@ -57,7 +79,7 @@ struct chan_ctx {
     chan::DevStatus *h_status = nullptr;
     int n1 = 0, n2 = 0, n3 = 0, px = 0, NJ = 0;
     long long plane = 0, vol = 0;
-    int ntx = 0, nty = 0, nchunks = 1, kchunk = 1;
+    int tile = CHAN_TILE_32x8, ntx = 0, nty = 0, nchunks = 1, kchunk = 1;   // stage-kernel launch shape
     int nstage = 2;
     int cur = 0;             // buffer holding the latest state
     bool uploaded = false;
@@ -83,6 +105,11 @@ struct chan_ctx {
     chan::DiagParams dp{};
     // fluctuation / Q-criterion buffers (allocated on first use)
     double *dq = nullptr, *dxyz = nullptr;
+    // ensemble membership: the device clock its graph replays read, and a
+    // counter of the kernel-visible settings, bumped by every call that
+    // changes them, so that an ensemble knows when its captured graph is stale
+    chan::DevClock *dclk = nullptr;
+    long long epoch = 0;
 };
 
 namespace {
@@ -195,6 +222,46 @@ void set_stage(chan_ctx *c, int iter)
     }
 }
 
+// stage-kernel launch shape: tile shape and number of k-chunks (0: the
+// chunk count whose CTAs fill whole waves of resident CTAs with the least
+// prologue overhead per marched plane)
+int set_launch(chan_ctx *c, int tile, int nchunks)
+{
+    if (tile < 0 || tile >= CHAN_NTILES) { c->err = "unknown tile shape"; return CHAN_EINVAL; }
+    const StageSet &ss = kStageSets[tile];
+    const int nz = c->n3 - 2;
+    if (nchunks < 0 || nchunks > nz) { c->err = "k-chunk count out of range"; return CHAN_EINVAL; }
+    const int ntx = (c->n1 - 2 + ss.ti - 1) / ss.ti, nty = (c->n2 - 2 + ss.tj - 1) / ss.tj;
+    if (nchunks == 0) {
+        int sms = 148, occ = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+        const int v = c->mixed ? 2 : 0;
+        CK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ss.k[0][v], ss.ti * ss.tj,
+                                                            v == 0 ? ss.smem : ss.smemf));
+        if (occ < 1) occ = 1;
+        const long long slots = (long long)sms * occ, tiles = (long long)ntx * nty;
+        double best = -1.0;
+        for (int nc = 1; nc <= nz; nc++) {
+            const int chunk = (nz + nc - 1) / nc;
+            if ((nz + chunk - 1) / chunk != nc) continue;
+            const long long ctas = tiles * nc;
+            const long long waves = (ctas + slots - 1) / slots;
+            const double eff = (double)ctas / (double)(waves * slots) * (double)chunk / (chunk + 2.5);
+            if (eff > best + 1e-9) { best = eff; nchunks = nc; }
+        }
+    }
+    // the chunk count that a chunk length of ceil(nz/nchunks) really gives
+    const int chunk = (nz + nchunks - 1) / nchunks;
+    c->tile = tile;
+    c->ntx = ntx;
+    c->nty = nty;
+    c->kchunk = chunk;
+    c->nchunks = (nz + chunk - 1) / chunk;
+    c->kp.kchunk = chunk;
+    c->epoch++;
+    return CHAN_OK;
+}
+
 int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
 {
     set_stage(c, iter);
@@ -205,17 +272,10 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
     const bool last = iter == c->nstage;
     {
         ProfScope ps(c, 0);
-        dim3 grid(c->ntx, c->nty, c->nchunks), block(TI, TJ);
-        const size_t smf = chan::StageShape<TI, TJ, float>::bytes;
-        if (!c->mixed)
-            chan::k_stage<TI, TJ, double, double, double>
-                <<<grid, block, chan::StageShape<TI, TJ, double>::bytes, c->stream>>>(c->kp);
-        else if (iter == 1)
-            chan::k_stage<TI, TJ, double, float, float><<<grid, block, smf, c->stream>>>(c->kp);
-        else if (last)
-            chan::k_stage<TI, TJ, float, double, float><<<grid, block, smf, c->stream>>>(c->kp);
-        else
-            chan::k_stage<TI, TJ, float, float, float><<<grid, block, smf, c->stream>>>(c->kp);
+        const StageSet &ss = kStageSets[c->tile];
+        dim3 grid(c->ntx, c->nty, c->nchunks), block(ss.ti, ss.tj);
+        const int v = !c->mixed ? 0 : (iter == 1 ? 1 : (last ? 3 : 2));
+        ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(c->kp);
     }
     CK(c, cudaGetLastError());
     {
@@ -268,24 +328,35 @@ int launch_diag(chan_ctx *c, long long step, double time)
     return CHAN_OK;
 }
 
-// queue nsteps steps; host counters advance optimistically
-int enqueue_steps(chan_ctx *c, int nsteps)
+// queue nsteps steps; host counters advance optimistically.  kCapture also
+// advances the device clock at the start of every step (for a graph whose
+// kernels read it); kCountOnly advances the host counters alone (after a
+// graph replay did the work).
+enum StepMode { kLaunch = 0, kCapture = 1, kCountOnly = 2 };
+int enqueue_steps(chan_ctx *c, int nsteps, int mode = kLaunch)
 {
     for (int s = 0; s < nsteps; s++) {
         const long long step = c->nstep + 1;
-        for (int it = 1; it <= c->nstage; it++) {
-            int r = launch_stage(c, it, it == c->nstage, step, c->time + c->p.dt);
-            if (r) return r;
+        if (mode == kCapture) {
+            chan::k_clock_advance<<<1, 32, 0, c->stream>>>(c->dclk, c->p.dt);
+            CK(c, cudaGetLastError());
         }
+        if (mode != kCountOnly)
+            for (int it = 1; it <= c->nstage; it++) {
+                int r = launch_stage(c, it, it == c->nstage, step, c->time + c->p.dt);
+                if (r) return r;
+            }
         c->nstep = step;
         c->time = c->time + c->p.dt;
-        if (c->diag_every > 0 && step % c->diag_every == 0) {
+        if (mode != kCountOnly && c->diag_every > 0 && step % c->diag_every == 0) {
             int r = launch_diag(c, step, c->time);
             if (r) return r;
         }
         if (c->p.istat > 0 && step % c->p.istat == 0) {
-            int r = launch_stats(c, step, 1, 1);
-            if (r) return r;
+            if (mode != kCountOnly) {
+                int r = launch_stats(c, step, 1, 1);
+                if (r) return r;
+            }
             if (c->kp.acc_on) {
                 if (c->tavg_samples == 0) c->tavg_t0 = c->time;
                 c->tavg_t1 = c->time;
@@ -579,54 +650,24 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     }
     k.force_on = p->forcing == CHAN_FORCE_WALLSHEAR ? 1 : 0;
     k.wall_custom = 0;
+    k.ri = 0.0; k.tref = 1.0; k.buoy_on = 0;
+    k.clk = nullptr;
     for (int w = 0; w < 2; w++) {
         k.wbc[w] = chan::WallBC{};
         k.wbc[w].Tw = p->Tw[w];
     }
 
-    // stage-kernel launch shape: tiles x k-chunks filling whole waves
-    c->ntx = (n1 - 2 + TI - 1) / TI;
-    c->nty = (n2 - 2 + TJ - 1) / TJ;
-    const size_t smem = chan::StageShape<TI, TJ, double>::bytes, smemf = chan::StageShape<TI, TJ, float>::bytes;
-    e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, double, double, double>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, double, float, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, float, float, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(chan::k_stage<TI, TJ, float, double, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemf);
+    // stage-kernel launch shape: the default tile, k-chunks filling whole waves
+    for (const StageSet &ss : kStageSets)
+        for (int b = 0; b < 2 && e == cudaSuccess; b++)
+            for (int v = 0; v < 4 && e == cudaSuccess; v++)
+                e = cudaFuncSetAttribute((const void *)ss.k[b][v], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(v == 0 ? ss.smem : ss.smemf));
     if (e != cudaSuccess) { fail(nullptr, "cudaFuncSetAttribute", e); chan_free(c); return CHAN_ECUDA; }
-    int sms = 148, occ = 1;
+    if (set_launch(c, CHAN_TILE_32x8, 0) != CHAN_OK) { g_init_error = c->err; chan_free(c); return CHAN_ECUDA; }
+    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
-    if (c->mixed)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ, float, float, float>, TI * TJ, smemf);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, chan::k_stage<TI, TJ, double, double, double>, TI * TJ,
-                                                      smem);
-    if (occ < 1) occ = 1;
-    const long long slots = (long long)sms * occ;
-    const int nz = n3 - 2;
-    const long long tiles = (long long)c->ntx * c->nty;
-    double best = -1.0;
-    int bestc = 1;
-    for (int nc = 1; nc <= nz; nc++) {
-        const int chunk = (nz + nc - 1) / nc;
-        const int nce = (nz + chunk - 1) / chunk;
-        if (nce != nc) continue;
-        const long long ctas = tiles * nc;
-        const long long waves = (ctas + slots - 1) / slots;
-        const double eff = (double)ctas / (double)(waves * slots) * (double)chunk / (chunk + 2.5);
-        if (eff > best + 1e-9) { best = eff; bestc = nc; }
-    }
-    c->nchunks = bestc;
     c->nsplit = stats_split(sms, n1, n2, n3);
-    c->kchunk = (nz + bestc - 1) / bestc;
-    k.kchunk = c->kchunk;
-
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { fail(nullptr, "init sync", e); chan_free(c); return CHAN_ECUDA; }
     *out = c;
@@ -916,8 +957,36 @@ int chan_checkpoint_read(chan_ctx *c, const char *path)
     CK(c, cudaStreamSynchronize(c->stream));
     c->nstep = h.nstep; c->time = h.time; c->sync_nstep = h.nstep; c->sync_time = h.time;
     c->tavg_samples = h.tavg_samples; c->tavg_t0 = h.tavg_t0; c->tavg_t1 = h.tavg_t1; c->kp.acc_on = h.acc_on;
+    c->epoch++;
     c->cur = 0;
     c->uploaded = true;
+    return CHAN_OK;
+}
+
+int chan_set_buoyancy(chan_ctx *c, double Ri, double Tref)
+{
+    if (!c) return CHAN_EINVAL;
+    if (!std::isfinite(Ri) || !std::isfinite(Tref)) { c->err = "Ri and Tref must be finite"; return CHAN_EINVAL; }
+    c->kp.ri = Ri;
+    c->kp.tref = Tref;
+    c->kp.buoy_on = Ri != 0.0 ? 1 : 0;
+    c->epoch++;
+    return CHAN_OK;
+}
+
+int chan_set_launch(chan_ctx *c, int32_t tile, int32_t nchunks)
+{
+    if (!c) return CHAN_EINVAL;
+    CK(c, cudaSetDevice(c->dev));
+    return set_launch(c, tile, nchunks);
+}
+
+int chan_get_launch(chan_ctx *c, int32_t *tile, int32_t *nchunks, int32_t *kchunk)
+{
+    if (!c) return CHAN_EINVAL;
+    if (tile) *tile = c->tile;
+    if (nchunks) *nchunks = c->nchunks;
+    if (kchunk) *kchunk = c->kchunk;
     return CHAN_OK;
 }
 
@@ -968,6 +1037,7 @@ int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc)
     c->kp.wall_custom = 0;
     for (int w = 0; w < 2; w++)
         if (c->kp.wbc[w].vel != 0 || c->kp.wbc[w].therm != 0) c->kp.wall_custom = 1;
+    c->epoch++;
     return CHAN_OK;
 }
 
@@ -979,6 +1049,7 @@ int chan_time_avg_start(chan_ctx *c)
     CK(c, cudaStreamSynchronize(c->stream));
     c->tavg_samples = 0;
     c->kp.acc_on = 1;
+    c->epoch++;
     return CHAN_OK;
 }
 
@@ -1251,6 +1322,398 @@ void chan_free(chan_ctx *c)
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: several contexts on one device stepped together.  Each member
+// keeps its own stream, buffers, parameters and launch shape.  A block of L
+// steps of every member (L = the least common multiple of their statistics
+// cadences, so that each replay starts at the same phase of every cadence) is
+// captured once into a CUDA graph with one branch per member; the graph is
+// replayed for as many whole blocks as a call asks for, and the members'
+// branches run concurrently, filling the GPU with small grids that alone
+// would not.  Kernels replayed from the graph read the step number and time
+// from a device clock per member (k_clock_advance moves it), since a graph's
+// kernel arguments are fixed at capture.  Results are bit for bit those of
+// stepping each member alone.
+
+struct chan_ensemble {
+    std::vector<chan_ctx *> m;
+    int dev = 0;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> join;
+    chan::DevClock *dclk = nullptr;   // [n] device clocks
+    chan::DevClock *hclk = nullptr;   // [n] pinned staging for the clock upload
+    cudaGraphExec_t exec = nullptr;
+    int L = 1;                        // steps per replay
+    std::vector<long long> cap_epoch, cap_phase;
+    long long replays = 0, captures = 0;
+    double last_ms = 0.0;             // device time of the last call's graph replays (CUDA events)
+    std::string err;
+};
+
+namespace {
+
+int efail(chan_ensemble *e, const char *what, cudaError_t r)
+{
+    e->err = std::string(what) + ": " + cudaGetErrorString(r);
+    return CHAN_ECUDA;
+}
+
+#define EK(e, call)                                    \
+    do {                                               \
+        cudaError_t r_ = (call);                       \
+        if (r_ != cudaSuccess) return efail((e), #call, r_); \
+    } while (0)
+
+long long gcd_ll(long long a, long long b)
+{
+    while (b) { const long long t = a % b; a = b; b = t; }
+    return a;
+}
+
+long long member_phase(const chan_ctx *c) { return c->p.istat > 0 ? c->nstep % c->p.istat : 0; }
+
+bool graph_valid(const chan_ensemble *e)
+{
+    if (!e->exec) return false;
+    for (size_t i = 0; i < e->m.size(); i++)
+        if (e->m[i]->epoch != e->cap_epoch[i] || member_phase(e->m[i]) != e->cap_phase[i]) return false;
+    return true;
+}
+
+// origin waits for every member's queued work; members wait for the origin
+int join_members_to_origin(chan_ensemble *e)
+{
+    for (size_t i = 0; i < e->m.size(); i++) {
+        EK(e, cudaEventRecord(e->join[i], e->m[i]->stream));
+        EK(e, cudaStreamWaitEvent(e->origin, e->join[i], 0));
+    }
+    return CHAN_OK;
+}
+int members_wait_origin(chan_ensemble *e)
+{
+    EK(e, cudaEventRecord(e->fork, e->origin));
+    for (chan_ctx *c : e->m) EK(e, cudaStreamWaitEvent(c->stream, e->fork, 0));
+    return CHAN_OK;
+}
+
+// capture L steps of every member into one graph (host counters restored)
+int build_graph(chan_ensemble *e)
+{
+    if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+    EK(e, cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+    int rc = CHAN_OK;
+    cudaError_t r = cudaEventRecord(e->fork, e->origin);
+    for (size_t i = 0; i < e->m.size() && rc == CHAN_OK && r == cudaSuccess; i++) {
+        chan_ctx *c = e->m[i];
+        r = cudaStreamWaitEvent(c->stream, e->fork, 0);
+        if (r != cudaSuccess) break;
+        const long long ns = c->nstep, tn = c->tavg_samples;
+        const double tm = c->time, ta = c->tavg_t0, tb = c->tavg_t1;
+        const int cur = c->cur;
+        const bool prof = c->prof;
+        c->prof = false;
+        c->kp.clk = c->dclk;
+        rc = enqueue_steps(c, e->L, kCapture);
+        if (rc != CHAN_OK) e->err = c->err;
+        c->kp.clk = nullptr;
+        c->prof = prof;
+        c->nstep = ns; c->time = tm; c->tavg_samples = tn; c->tavg_t0 = ta; c->tavg_t1 = tb; c->cur = cur;
+        if (rc == CHAN_OK) r = cudaEventRecord(e->join[i], c->stream);
+        if (rc == CHAN_OK && r == cudaSuccess) r = cudaStreamWaitEvent(e->origin, e->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t re = cudaStreamEndCapture(e->origin, &g);
+    if (rc != CHAN_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (r != cudaSuccess) { if (g) cudaGraphDestroy(g); return efail(e, "capture", r); }
+    if (re != cudaSuccess) return efail(e, "cudaStreamEndCapture", re);
+    const cudaError_t ri = cudaGraphInstantiate(&e->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ri != cudaSuccess) { e->exec = nullptr; return efail(e, "cudaGraphInstantiate", ri); }
+    for (size_t i = 0; i < e->m.size(); i++) {
+        e->cap_epoch[i] = e->m[i]->epoch;
+        e->cap_phase[i] = member_phase(e->m[i]);
+    }
+    e->captures++;
+    return CHAN_OK;
+}
+
+// one timed trial of the autotuner: every stage but the last of every
+// member, reps times, all members concurrently; the state is not modified
+// (only the stage buffers and the wall ring, which the caller restores)
+int tune_trial(chan_ensemble *e, int reps, float *ms)
+{
+    int rc = members_wait_origin(e);
+    if (rc) return rc;
+    EK(e, cudaEventRecord(e->t0, e->origin));
+    rc = members_wait_origin(e);
+    if (rc) return rc;
+    for (chan_ctx *c : e->m) {
+        const int ns = c->nstage > 1 ? c->nstage - 1 : 1;
+        for (int r = 0; r < reps; r++)
+            for (int it = 1; it <= ns; it++) {
+                rc = launch_stage(c, it, false, c->nstep + 1, c->time + c->p.dt);
+                if (rc) { e->err = c->err; return rc; }
+            }
+    }
+    rc = join_members_to_origin(e);
+    if (rc) return rc;
+    EK(e, cudaEventRecord(e->t1, e->origin));
+    EK(e, cudaEventSynchronize(e->t1));
+    EK(e, cudaEventElapsedTime(ms, e->t0, e->t1));
+    *ms /= (float)reps;
+    return CHAN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chan_ensemble_create(chan_ctx *const *members, int32_t n, chan_ensemble **out)
+{
+    if (!members || n < 1 || !out) return CHAN_EINVAL;
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!members[i] || members[i]->dclk) return CHAN_EINVAL;   // null, or already in an ensemble
+        for (int j = 0; j < i; j++)
+            if (members[j] == members[i]) return CHAN_EINVAL;
+        if (members[i]->dev != members[0]->dev) return CHAN_EINVAL;
+    }
+    long long L = 1;
+    for (int i = 0; i < n; i++) {
+        const long long is = members[i]->p.istat > 0 ? members[i]->p.istat : 1;
+        L = L / gcd_ll(L, is) * is;
+        if (L > 10000) return CHAN_EINVAL;   // statistics cadences too far apart for one graph block
+    }
+    chan_ensemble *e = new chan_ensemble;
+    e->m.assign(members, members + n);
+    e->dev = members[0]->dev;
+    e->L = (int)L;
+    e->join.assign(n, nullptr);
+    e->cap_epoch.assign(n, -1);
+    e->cap_phase.assign(n, -1);
+    cudaError_t r = cudaSetDevice(e->dev);
+    if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking);
+    if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    if (r == cudaSuccess) r = cudaEventCreate(&e->t0);
+    if (r == cudaSuccess) r = cudaEventCreate(&e->t1);
+    for (int i = 0; i < n && r == cudaSuccess; i++) r = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+    if (r == cudaSuccess) r = cudaMalloc((void **)&e->dclk, n * sizeof(chan::DevClock));
+    if (r == cudaSuccess) r = cudaMallocHost((void **)&e->hclk, n * sizeof(chan::DevClock));
+    if (r != cudaSuccess) {
+        g_init_error = std::string("chan_ensemble_create: ") + cudaGetErrorString(r);
+        chan_ensemble_free(e);
+        return CHAN_ECUDA;
+    }
+    for (int i = 0; i < n; i++) e->m[i]->dclk = e->dclk + i;
+    *out = e;
+    return CHAN_OK;
+}
+
+int chan_ensemble_size(chan_ensemble *e) { return e ? (int)e->m.size() : 0; }
+
+int chan_ensemble_block(chan_ensemble *e) { return e ? e->L : 0; }
+
+int chan_ensemble_step(chan_ensemble *e, int32_t nsteps, int32_t *status)
+{
+    if (!e || nsteps < 0) return CHAN_EINVAL;
+    for (chan_ctx *c : e->m) {
+        if (!c->uploaded) { e->err = "member not uploaded"; return CHAN_ESTATE; }
+        if (c->diag_every > 0) { e->err = "members step without the diagnostics series"; return CHAN_ESTATE; }
+    }
+    EK(e, cudaSetDevice(e->dev));
+    int rc = join_members_to_origin(e);
+    if (rc) return rc;
+    int left = nsteps;
+    bool timed = false;
+    if (left >= e->L) {
+        if (!graph_valid(e)) {
+            rc = build_graph(e);
+            if (rc) return rc;
+        }
+        for (size_t i = 0; i < e->m.size(); i++) e->hclk[i] = chan::DevClock{e->m[i]->nstep, e->m[i]->time};
+        EK(e, cudaMemcpyAsync(e->dclk, e->hclk, e->m.size() * sizeof(chan::DevClock), cudaMemcpyHostToDevice,
+                              e->origin));
+        EK(e, cudaEventRecord(e->t0, e->origin));
+        while (left >= e->L) {
+            EK(e, cudaGraphLaunch(e->exec, e->origin));
+            for (chan_ctx *c : e->m) enqueue_steps(c, e->L, kCountOnly);
+            e->replays++;
+            left -= e->L;
+        }
+        EK(e, cudaEventRecord(e->t1, e->origin));
+        timed = true;
+    }
+    rc = members_wait_origin(e);
+    if (rc) return rc;
+    int first = CHAN_OK;
+    for (size_t i = 0; i < e->m.size(); i++) {
+        chan_ctx *c = e->m[i];
+        int r = left > 0 ? enqueue_steps(c, left) : CHAN_OK;
+        if (r == CHAN_OK) r = read_status(c, nullptr);
+        if (status) status[i] = r;
+        if (r != CHAN_OK && first == CHAN_OK) first = r;
+    }
+    // the pinned clock staging is reused by the next call: it has been read
+    EK(e, cudaStreamSynchronize(e->origin));
+    e->last_ms = 0.0;
+    if (timed) {
+        float ms = 0.f;
+        EK(e, cudaEventElapsedTime(&ms, e->t0, e->t1));
+        e->last_ms = ms;
+    }
+    return first;
+}
+
+int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
+{
+    if (!e || reps < 1) return CHAN_EINVAL;
+    for (chan_ctx *c : e->m)
+        if (!c->uploaded) { e->err = "member not uploaded"; return CHAN_ESTATE; }
+    EK(e, cudaSetDevice(e->dev));
+    const size_t n = e->m.size();
+    // the wall ring and the status are the only persistent device state the
+    // trial stages write: keep copies and put them back afterwards
+    std::vector<double *> wsave(n, nullptr);
+    std::vector<chan::DevStatus *> ssave(n, nullptr);
+    std::vector<int> cur(n);
+    std::vector<int> tile(n), nch(n);
+    int rc = join_members_to_origin(e);
+    for (size_t i = 0; i < n && rc == CHAN_OK; i++) {
+        chan_ctx *c = e->m[i];
+        const size_t nw = 2 * 8 * (size_t)c->plane;
+        cudaError_t r = cudaMalloc((void **)&wsave[i], nw * sizeof(double));
+        if (r == cudaSuccess) r = cudaMalloc((void **)&ssave[i], sizeof(chan::DevStatus));
+        if (r == cudaSuccess) r = cudaMemcpyAsync(wsave[i], c->wp, nw * sizeof(double), cudaMemcpyDeviceToDevice,
+                                                  e->origin);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(ssave[i], c->status, sizeof(chan::DevStatus),
+                                                  cudaMemcpyDeviceToDevice, e->origin);
+        if (r != cudaSuccess) rc = efail(e, "tune: save", r);
+        cur[i] = c->cur;
+        tile[i] = c->tile;
+        nch[i] = c->nchunks;
+    }
+    // candidate shapes of one member: each tile shape at several k-chunk depths
+    auto candidates = [](const chan_ctx *c) {
+        std::vector<std::pair<int, int>> v;
+        const int nz = c->n3 - 2;
+        const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
+        for (int t = 0; t < CHAN_NTILES; t++) {
+            int last = -1;
+            for (int d : depth) {
+                const int nc = std::max(1, (nz + std::min(d, nz) - 1) / std::min(d, nz));
+                const int chunk = (nz + nc - 1) / nc, real = (nz + chunk - 1) / chunk;
+                if (real != last) v.push_back({t, real});
+                last = real;
+            }
+        }
+        return v;
+    };
+    auto apply = [&](const std::vector<int> &t, const std::vector<int> &c) {
+        for (size_t i = 0; i < n; i++) {
+            const int r = set_launch(e->m[i], t[i], c[i]);
+            if (r) { e->err = e->m[i]->err; return r; }
+        }
+        return (int)CHAN_OK;
+    };
+    float best = 0.f, ms = 0.f;
+    if (rc == CHAN_OK) rc = tune_trial(e, reps, &ms);   // warm-up of the current shapes
+    if (rc == CHAN_OK) rc = tune_trial(e, reps, &best);
+    // 1. one shape for every member: each tile shape at each k-chunk depth
+    if (rc == CHAN_OK) {
+        const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
+        for (int t = 0; t < CHAN_NTILES && rc == CHAN_OK; t++)
+            for (int d : depth) {
+                std::vector<int> tt(n, t), cc(n);
+                for (size_t i = 0; i < n; i++) {
+                    const int nz = e->m[i]->n3 - 2, dd = std::min(d, nz);
+                    cc[i] = (nz + dd - 1) / dd;
+                }
+                rc = apply(tt, cc);
+                if (rc == CHAN_OK) rc = tune_trial(e, reps, &ms);
+                if (rc != CHAN_OK) break;
+                if (ms < best) { best = ms; tile = tt; nch = cc; }
+            }
+    }
+    // 2. one pass of per-member refinement, largest members first
+    if (rc == CHAN_OK) {
+        std::vector<size_t> order(n);
+        for (size_t i = 0; i < n; i++) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return e->m[a]->vol > e->m[b]->vol; });
+        for (size_t oi = 0; oi < n && rc == CHAN_OK; oi++) {
+            const size_t i = order[oi];
+            for (auto cand : candidates(e->m[i])) {
+                if (cand.first == tile[i] && cand.second == nch[i]) continue;
+                std::vector<int> tt = tile, cc = nch;
+                tt[i] = cand.first;
+                cc[i] = cand.second;
+                rc = apply(tt, cc);
+                if (rc == CHAN_OK) rc = tune_trial(e, reps, &ms);
+                if (rc != CHAN_OK) break;
+                if (ms < best * 0.995f) { best = ms; tile = tt; nch = cc; }
+            }
+        }
+    }
+    int ra = apply(tile, nch);
+    if (rc == CHAN_OK) rc = ra;
+    // restore the wall rings, statuses and buffer roles
+    for (size_t i = 0; i < n; i++) {
+        chan_ctx *c = e->m[i];
+        if (wsave[i] && ssave[i]) {
+            cudaError_t r = cudaMemcpyAsync(c->wp, wsave[i], 2 * 8 * (size_t)c->plane * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, e->origin);
+            if (r == cudaSuccess)
+                r = cudaMemcpyAsync(c->status, ssave[i], sizeof(chan::DevStatus), cudaMemcpyDeviceToDevice, e->origin);
+            if (r != cudaSuccess && rc == CHAN_OK) rc = efail(e, "tune: restore", r);
+        }
+        c->cur = cur[i];
+    }
+    cudaError_t r = cudaStreamSynchronize(e->origin);
+    if (r != cudaSuccess && rc == CHAN_OK) rc = efail(e, "tune: sync", r);
+    for (size_t i = 0; i < n; i++) {
+        if (wsave[i]) cudaFree(wsave[i]);
+        if (ssave[i]) cudaFree(ssave[i]);
+    }
+    if (rc == CHAN_OK) {
+        const int rm = members_wait_origin(e);
+        if (rm) rc = rm;
+    }
+    if (best_ms) *best_ms = best;
+    return rc;
+}
+
+int chan_ensemble_counters(chan_ensemble *e, int64_t *replays, int64_t *captures, double *last_ms)
+{
+    if (!e) return CHAN_EINVAL;
+    if (replays) *replays = e->replays;
+    if (captures) *captures = e->captures;
+    if (last_ms) *last_ms = e->last_ms;
+    return CHAN_OK;
+}
+
+const char *chan_ensemble_last_error(chan_ensemble *e) { return e ? e->err.c_str() : g_init_error.c_str(); }
+
+void chan_ensemble_free(chan_ensemble *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->dev);
+    if (e->origin) cudaStreamSynchronize(e->origin);
+    for (chan_ctx *c : e->m)
+        if (c && c->dclk >= e->dclk && c->dclk < e->dclk + e->m.size()) c->dclk = nullptr;
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    for (cudaEvent_t j : e->join)
+        if (j) cudaEventDestroy(j);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->t0) cudaEventDestroy(e->t0);
+    if (e->t1) cudaEventDestroy(e->t1);
+    if (e->dclk) cudaFree(e->dclk);
+    if (e->hclk) cudaFreeHost(e->hclk);
+    if (e->origin) cudaStreamDestroy(e->origin);
+    delete e;
 }
 
 }  // extern "C"

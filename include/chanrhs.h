@@ -218,6 +218,27 @@ typedef struct chan_wall_bc {
 } chan_wall_bc;
 int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc);
 
+/* Stage-kernel launch shape (no reference counterpart; it changes no result
+ * bits).  tile: CHAN_TILE_32x8 (256 threads, the default) or CHAN_TILE_32x4
+ * (128 threads) columns x rows per CTA; nchunks: how many CTAs split the
+ * wall-normal march of one tile column (1..nP3-2; 0 picks the count that fills
+ * whole waves of resident CTAs, as chan_init does).  chan_get_launch reports
+ * the shape in use and the planes per chunk. */
+#define CHAN_TILE_32x8 0
+#define CHAN_TILE_32x4 1
+#define CHAN_NTILES 2
+int chan_set_launch(chan_ctx *c, int32_t tile, int32_t nchunks);
+int chan_get_launch(chan_ctx *c, int32_t *tile, int32_t *nchunks, int32_t *kchunk);
+
+/* Buoyancy body force for stratified runs (no reference counterpart: the
+ * reference's stratified variants v1.9_strat change only the wall
+ * temperature).  Adds, at every interior point,
+ *     S(rho*w) = Ri * rho * (T - Tref),   S(rho*E) = ggM * w * S(rho*w)
+ * to the right-hand side, w the wall-normal velocity (gravity along -x3) and
+ * ggM = gama*(gama-1)*Mac^2 the energy scaling of the forcing term
+ * (main_v1.9.f90:565-571).  Ri = 0 (the default) switches it off. */
+int chan_set_buoyancy(chan_ctx *c, double Ri, double Tref);
+
 /* Exact binary checkpoint of a context's device state between time steps:
  * the conservative state with its periodic ghosts, both wall planes, the
  * corner columns, the forcing/statistics state and the step counter, time and
@@ -323,8 +344,55 @@ int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const 
  * memory checker in tests; the reference has no counterpart. */
 int chan_debug_canaries(chan_ctx *c, int64_t *corrupted);
 
-/* Free device memory and the context.  NULL is allowed. */
+/* Free device memory and the context.  NULL is allowed.  A context that is a
+ * member of an ensemble is freed after its ensemble. */
 void chan_free(chan_ctx *c);
+
+/* ------------------------------------------------------------------------
+ * Ensembles (no reference counterpart: the reference runs one case per MPI
+ * job).  Several contexts on one device -- a parameter sweep of cases with
+ * their own grids, physics, wall BCs and precision -- stepped together.
+ * Every member keeps its own buffers and stream.  A block of L steps of all
+ * members (L = least common multiple of their istat) is captured once into
+ * one CUDA graph, one branch per member, and replayed; the members' kernels
+ * run concurrently.  Each member's results are bit for bit those of
+ * chan_step on that member alone.  A context belongs to one ensemble at most;
+ * members may still be used on their own between ensemble calls. */
+typedef struct chan_ensemble chan_ensemble;
+
+/* members: n distinct contexts on one device.  CHAN_EINVAL if a member is
+ * NULL, repeated, already in an ensemble, on another device, or if L would
+ * exceed 10000 steps. */
+int chan_ensemble_create(chan_ctx *const *members, int32_t n, chan_ensemble **out);
+int chan_ensemble_size(chan_ensemble *e);
+/* L, the steps per graph replay */
+int chan_ensemble_block(chan_ensemble *e);
+
+/* nsteps whole steps of every member: graph replays for the whole blocks of
+ * L steps, then the remaining steps queued on the members' own streams; each
+ * member's per-step tail (statistics every istat, time averaging) as in
+ * chan_step.  Waits, then reads every member's status into status[n] (may be
+ * NULL) and returns the first nonzero one.  Members must be uploaded and
+ * must not have the diagnostics series enabled. */
+int chan_ensemble_step(chan_ensemble *e, int32_t nsteps, int32_t *status);
+
+/* Autotuner of the members' stage-kernel launch shapes (chan_set_launch).
+ * It times, with CUDA events, all but the last RK stage of every member run
+ * concurrently, reps times per trial: first one shape for every member (each
+ * tile shape at k-chunk depths of 4 to 128 planes and the whole height),
+ * then one pass that tries every candidate for each member in turn, largest
+ * grids first, keeping a change that saves more than 0.5%.  The members'
+ * states, wall rings, statuses and counters are left as they were.  Writes
+ * the best trial time (ms per trial step) to best_ms. */
+int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms);
+
+/* graph replays and graph captures so far, and the device time (CUDA events
+ * on the launching stream) of the graph replays of the last
+ * chan_ensemble_step call (0 if it replayed none) */
+int chan_ensemble_counters(chan_ensemble *e, int64_t *replays, int64_t *captures, double *last_ms);
+const char *chan_ensemble_last_error(chan_ensemble *e);
+/* Frees the ensemble (not its members).  NULL is allowed. */
+void chan_ensemble_free(chan_ensemble *e);
 
 #ifdef __cplusplus
 }

@@ -80,6 +80,8 @@ typedef struct {
     double wTw[2], wdTdz[2], wg[2], wwave[2][4];
     unsigned char *wmask[2];
     double *wuv[2], *wx1[2];
+    /* buoyancy body force (orc_set_buoyancy); ri = 0: off */
+    double ri, tref;
 } orc_t;
 
 #define ID(o, i, j, k) ((((size_t)(k)) * (o)->NJ + (size_t)(j)) * (o)->NI + (size_t)(i))
@@ -307,6 +309,12 @@ void orc_upload(orc_t *o, const double *v, long nstep, double time)
 }
 
 /* Forcing state (the lagged wall shear and plane-mean density) */
+void orc_set_buoyancy(orc_t *o, double ri, double tref)
+{
+    o->ri = ri;
+    o->tref = tref;
+}
+
 void orc_set_forcing(orc_t *o, double tauL, double tauU, const double *rhobar)
 {
     int k;
@@ -501,6 +509,13 @@ void orc_stage(orc_t *o, int iter)
                     src[2] = force ? fcoef * o->stat1[k - 1] : zer;
                     src[3] = zer; src[4] = zer;
                     src[5] = force ? ggM * VAR(o, 2, i, j, k) * haf * (o->tauL - o->tauU) * o->stat1[k - 1] : zer;
+                    if (o->ri != zer) {
+                        /* buoyancy ri*rho*(T - tref) on rho*w (w wall-normal, gravity along -x3)
+                         * and its work ggM*w*(that) on rho*E; no reference counterpart */
+                        const double bq = o->ri * (VAR(o, 1, i, j, k) * (VAR(o, 6, i, j, k) - o->tref));
+                        src[4] = bq;
+                        src[5] = src[5] + (ggM * VAR(o, 4, i, j, k)) * bq;
+                    }
                     for (m = 1; m <= 5; m++) {
                         F2 = (FD(o, m, i + 1, j, k) - FD(o, m, i - 1, j, k)) * haf * invdx;
                         G2 = (GD(o, m, i, j + 1, k) - GD(o, m, i, j - 1, k)) * haf * invdy;

@@ -67,6 +67,7 @@ def lib():
         L.orc_download_solv.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
         L.orc_get_stats.argtypes = [ctypes.c_void_p, _D, _D, _D, _D]
         L.orc_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D]
+        L.orc_set_buoyancy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.orc_set_wall_bc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, _D, ctypes.c_void_p, _D, _D]
         L.orc_diagnostics.argtypes = [_D, _I, _I, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, _D]
@@ -184,6 +185,10 @@ class Oracle:
     def set_forcing(self, tauL, tauU, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         lib().orc_set_forcing(self._h, float(tauL), float(tauU), _dp(rb))
+
+    def set_buoyancy(self, Ri, Tref=1.0):
+        """Same buoyancy body force as Channel.set_buoyancy."""
+        lib().orc_set_buoyancy(self._h, float(Ri), float(Tref))
 
     def set_wall_bc(self, wall, bc):
         """Same WallBC description as Channel.set_wall_bc."""

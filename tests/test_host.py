@@ -206,3 +206,32 @@ def test_mixed_check_rejects_bad_windows_before_any_device_work():
     for steps, avg_from, every in ((1000, 500, 300), (1000, 1000, 100), (1000, 200, 15), (950, 100, 100)):
         with pytest.raises(ValueError):
             mixed_check.compare(p, None, None, None, None, steps, avg_from, every)
+
+
+def test_sweep_cases_cover_the_parameter_grid_and_are_seeded():
+    from compchan3dmpi_b200.ensemble import sweep_cases, sweep_grids, MACH, REYNOLDS, RICHARDSON, DELTA_T
+    g = sweep_grids(16)
+    assert g[0] == (64, 64, 65)
+    assert max(n[0] for n in g) == 160 and max(n[1] for n in g) == 128 and max(n[2] for n in g) == 129
+    assert len(set(g)) == 16 and all(n[2] % 2 == 1 for n in g)
+    a = sweep_cases(16, grids=[(24, 16, 17)] * 16)
+    b = sweep_cases(16, grids=[(24, 16, 17)] * 16)
+    combos = {(c.params.Mac, c.params.Re, c.Ri, c.dT) for c in a}
+    assert len(combos) == 16          # drawn without repetition
+    for c in a:
+        assert c.params.Mac in MACH and c.params.Re in REYNOLDS and c.Ri in RICHARDSON and c.dT in DELTA_T
+        assert c.params.Tw == (1.0 - 0.5 * c.dT, 1.0 + 0.5 * c.dT)
+        assert c.params.mixed and c.params.dt > 0
+    for x, y in zip(a, b):
+        assert np.array_equal(x.var, y.var) and x.params == y.params
+
+
+def test_stratified_start_is_at_uniform_pressure():
+    from compchan3dmpi_b200.ensemble import stratified_start
+    p = ChanParams(nP=(12, 10, 13), Tw=(0.9, 1.1))
+    x3, jac, inv = mesh_tanh(13, 2.2)
+    v = stratified_start(p, x3, 0.9, 1.1, seed=5)
+    assert np.allclose(v[5][0], 0.9) and np.allclose(v[5][-1], 1.1)
+    assert np.allclose(v[6], 1.0 / (p.gama * p.Mac ** 2))
+    assert np.allclose(v[0] * v[5], 1.0)
+    assert np.allclose(v[4], v[5] + 0.5 * p.ggM * (v[1] ** 2 + v[2] ** 2 + v[3] ** 2))

@@ -127,3 +127,33 @@ def test_plane_mass_conserved_by_one_scheme():
     o.stage(1)
     rel = np.abs(plane_mass(o.download())[1:-1] - plane_mass(var)[1:-1]) / plane_mass(var)[1:-1]
     assert rel.max() > 1e-12    # the hybrid switch is not conservative
+
+
+def test_oracle_buoyancy_source_is_the_stated_term():
+    """One RK2 first stage (Q <- Q + dt/2 R) with and without the buoyancy
+    term: rho*w changes by dt/2*Ri*rho*(T - Tref) and rho*E by ggM*w times
+    that; rho, rho*u and rho*v are untouched, bit for bit."""
+    from chan_cases import make_case
+    p, x3, jac, inv, var = make_case(nP=(12, 10, 13), quantize=False)
+    p = p.with_(Tw=(0.9, 1.1))
+    Ri, Tref = 0.5, 1.05
+    a = O.Oracle(p, x3, jac, inv, threads=1)
+    b = O.Oracle(p, x3, jac, inv, threads=1)
+    b.set_buoyancy(Ri, Tref)
+    for o in (a, b):
+        o.upload(var)
+        o.stage(1)
+    qa, qb = a.download_solv(0), b.download_solv(0)
+    a.close(); b.close()
+    n1, n2, n3 = p.nP
+    sl = (slice(1, n3 - 1), slice(1, n2 - 1), slice(1, n1 - 1))   # interior k, j, i (0-based)
+    rho, w, T = var[0][sl], var[3][sl], var[5][sl]
+    bq = Ri * (rho * (T - Tref))
+    cdt = 0.5 * p.dt
+    for m in (0, 1, 2):
+        assert np.array_equal(qa[m][sl], qb[m][sl]), m
+    dw = qb[3][sl] - qa[3][sl]
+    dE = qb[4][sl] - qa[4][sl]
+    assert np.max(np.abs(bq)) > 1e-3
+    assert np.max(np.abs(dw - cdt * bq)) <= 1e-12 * np.max(np.abs(qa[3][sl])) + 1e-15
+    assert np.max(np.abs(dE - cdt * p.ggM * w * bq)) <= 1e-12 * np.max(np.abs(qa[4][sl])) + 1e-15
