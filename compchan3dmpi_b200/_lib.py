@@ -116,7 +116,8 @@ SIGNATURES = [
 
 CHAN_TILE_32x8 = 0
 CHAN_TILE_32x4 = 1
-CHAN_NTILES = 2
+CHAN_TILE_16x16 = 2
+CHAN_NTILES = 3
 
 _lib = None
 

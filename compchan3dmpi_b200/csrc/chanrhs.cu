@@ -45,8 +45,9 @@ StageSet make_stage_set()
     s.smemf = chan::StageShape<TI_, TJ_, float>::bytes;
     return s;
 }
-// CHAN_TILE_32x8 (default) and CHAN_TILE_32x4
-const StageSet kStageSets[CHAN_NTILES] = {make_stage_set<32, 8>(), make_stage_set<32, 4>()};
+// CHAN_TILE_32x8 (default), CHAN_TILE_32x4, CHAN_TILE_16x16
+const StageSet kStageSets[CHAN_NTILES] = {make_stage_set<32, 8>(), make_stage_set<32, 4>(),
+                                          make_stage_set<16, 16>()};
 constexpr int kMaxSplit = 16;   // statistics blocks per plane, at most
 
 std::string g_init_error;
