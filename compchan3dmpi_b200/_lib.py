@@ -21,6 +21,7 @@ CHAN_MIXED = 1
 _D = ctypes.POINTER(ctypes.c_double)
 _I32 = ctypes.POINTER(ctypes.c_int32)
 _I64 = ctypes.POINTER(ctypes.c_int64)
+_F = ctypes.POINTER(ctypes.c_float)
 
 
 class ChanWallBCC(ctypes.Structure):
@@ -112,6 +113,30 @@ SIGNATURES = [
     ("chan_ensemble_counters", ctypes.c_int, [ctypes.c_void_p, _I64, _I64, _D]),
     ("chan_ensemble_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("chan_ensemble_free", None, [ctypes.c_void_p]),
+    ("chan_selftest_umma", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16),
+                                          ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int32]),
+    ("chan_closure_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("chan_closure_sample", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_int32, _I64]),
+    ("chan_closure_add_data", ctypes.c_int, [ctypes.c_void_p, _F, _F, ctypes.c_int64]),
+    ("chan_closure_count", ctypes.c_int, [ctypes.c_void_p, _I64]),
+    ("chan_closure_get_data", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, _F, _F]),
+    ("chan_closure_fit_normalization", ctypes.c_int, [ctypes.c_void_p, _F]),
+    ("chan_closure_set_normalization", ctypes.c_int, [ctypes.c_void_p, _F]),
+    ("chan_closure_get_normalization", ctypes.c_int, [ctypes.c_void_p, _F]),
+    ("chan_closure_nparams", ctypes.c_int, []),
+    ("chan_closure_init", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("chan_closure_set_params", ctypes.c_int, [ctypes.c_void_p, _F]),
+    ("chan_closure_get_params", ctypes.c_int, [ctypes.c_void_p, _F]),
+    ("chan_closure_train", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                          ctypes.c_uint64, _D]),
+    ("chan_closure_grad", ctypes.c_int, [ctypes.c_void_p, _F, _F, ctypes.c_int64, _F, _D]),
+    ("chan_closure_infer", ctypes.c_int, [ctypes.c_void_p, _F, ctypes.c_int64, _F]),
+    ("chan_closure_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("chan_closure_free", None, [ctypes.c_void_p]),
+    ("chan_set_closure", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
+    ("chan_closure_flag", ctypes.c_int, [ctypes.c_void_p, _I32, ctypes.c_int32]),
 ]
 
 CHAN_TILE_32x8 = 0

@@ -24,7 +24,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 
 
 def sources():
-    return [SRC / "chanrhs.cu", SRC / "deck_io.cpp"]
+    return [SRC / "chanrhs.cu", SRC / "closure.cu", SRC / "deck_io.cpp"]
 
 
 def deps():

@@ -1512,6 +1512,190 @@ __global__ void k_check(const KParams P, const double *q)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Learned subgrid closure: features, filtered-DNS targets, and the closure
+// source.  No reference counterpart (the reference resolves every scale).
+
+constexpr int kSgsIn = 13, kSgsOut = 9;   // closure features and fluxes per point
+
+// periodic image of any x or spanwise index on the unique points 2..n-1
+__device__ __forceinline__ int wrap_any(int i, int n)
+{
+    const int m = n - 2;
+    int r = (i - 2) % m;
+    if (r < 0) r += m;
+    return r + 2;
+}
+
+// primitives (rho, u, v, w, T) at (i, j, k): the wall-plane ring on the
+// walls, the conservative state elsewhere (exact divisions)
+__device__ __forceinline__ void prim_at(const KParams &P, const double *q, int i, int j, int k, double x[5])
+{
+    i = wrap_any(i, P.n1);
+    j = wrap_any(j, P.n2);
+    if (k <= 1 || k >= P.n3) {
+        const double *W = P.wp + (size_t)(k <= 1 ? 0 : 8) * P.plane + (long long)j * P.px + i;
+        x[0] = W[0]; x[1] = W[P.plane]; x[2] = W[2 * P.plane]; x[3] = W[3 * P.plane]; x[4] = W[5 * P.plane];
+        return;
+    }
+    const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+    const double r = q[o];
+    x[0] = r;
+    x[1] = q[P.vol + o] / r;
+    x[2] = q[2 * P.vol + o] / r;
+    x[3] = q[3 * P.vol + o] / r;
+    x[4] = q[4 * P.vol + o] / r - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
+}
+
+// Favre-filtered (rho, u, v, w, T) at (i, j, k): a box of width fw (even)
+// in x and spanwise, the trapezoid weights (1/2, 1, .., 1, 1/2) / fw per
+// direction; fw = 0 returns the point's own values.  With prod != 0 it also
+// returns the filtered rho*u_a*u_b (uu, vv, ww, uv, uw, vw) and rho*u_b*T.
+__device__ __forceinline__ void favre_at(const KParams &P, const double *q, int i, int j, int k, int fw,
+                                         double f[5], double *prod)
+{
+    if (fw == 0) {
+        prim_at(P, q, i, j, k, f);
+        if (prod) {
+            const double r = f[0], u = f[1], v = f[2], w = f[3], T = f[4];
+            prod[0] = r * u * u; prod[1] = r * v * v; prod[2] = r * w * w;
+            prod[3] = r * u * v; prod[4] = r * u * w; prod[5] = r * v * w;
+            prod[6] = r * u * T; prod[7] = r * v * T; prod[8] = r * w * T;
+        }
+        return;
+    }
+    const int h = fw / 2;
+    double sr = 0, su = 0, sv = 0, sw = 0, sT = 0, sp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = -h; b <= h; b++) {
+        const double wb = (b == -h || b == h) ? 0.5 : 1.0;
+        for (int a = -h; a <= h; a++) {
+            const double wgt = wb * ((a == -h || a == h) ? 0.5 : 1.0);
+            double x[5];
+            prim_at(P, q, i + a, j + b, k, x);
+            const double r = x[0], u = x[1], v = x[2], w = x[3], T = x[4], rw = wgt * r;
+            sr += wgt * r; su += rw * u; sv += rw * v; sw += rw * w; sT += rw * T;
+            if (prod) {
+                sp[0] += rw * u * u; sp[1] += rw * v * v; sp[2] += rw * w * w;
+                sp[3] += rw * u * v; sp[4] += rw * u * w; sp[5] += rw * v * w;
+                sp[6] += rw * u * T; sp[7] += rw * v * T; sp[8] += rw * w * T;
+            }
+        }
+    }
+    const double nrm = 1.0 / ((double)fw * (double)fw);
+    f[0] = sr * nrm;
+    f[1] = su / sr; f[2] = sv / sr; f[3] = sw / sr; f[4] = sT / sr;
+    if (prod)
+        for (int c = 0; c < 9; c++) prod[c] = sp[c] * nrm;
+}
+
+struct SgsSampling {
+    int sx, sy, sz, fw;          // gradient strides, filter width
+    int i0, ni, j0, nj, k0, nk;  // sample points i0 + sx*a (a < ni), j0 + sy*b, k0 + sz*c
+    const double *x3;            // x3(1..nP3) at x3[k-1]
+    float *X, *T;                // [n][13], [n][9] (T may be null)
+};
+
+// Features (and with T the filtered subgrid fluxes) at every sample point.
+// Gradients by central differences of the filtered fields at the sample
+// strides (the coarse grid's spacing); y+ from the wall shear of the last
+// statistics step.
+__global__ void k_sgs_sample(const KParams P, const double *q, const SgsSampling S)
+{
+    const long long n = (long long)S.ni * S.nj * S.nk;
+    const double Lx = 1.0 / P.invdx, Ly = 1.0 / P.invdy;   // dx, dy
+    const int n3 = P.n3;
+    const double tw = 0.5 * (P.stat[23 * n3] - P.stat[23 * n3 + 1]);
+    const double rw = 0.5 * (P.stat[0] + P.stat[n3 - 1]);
+    // before the first statistics step the sums are zero: y+ is then 0
+    const double ut = rw > 0.0 ? sqrt(fmax(tw, 0.0) / rw) : 0.0, muw = 0.5 * (P.muwb + P.muwt);
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(s % S.ni), b = (int)((s / S.ni) % S.nj), c = (int)(s / ((long long)S.ni * S.nj));
+        const int i = S.i0 + S.sx * a, j = S.j0 + S.sy * b, k = S.k0 + S.sz * c;
+        double f0[5], prod[9], fxp[5], fxm[5], fyp[5], fym[5], fzp[5], fzm[5];
+        favre_at(P, q, i, j, k, S.fw, f0, S.T ? prod : nullptr);
+        favre_at(P, q, i + S.sx, j, k, S.fw, fxp, nullptr);
+        favre_at(P, q, i - S.sx, j, k, S.fw, fxm, nullptr);
+        favre_at(P, q, i, j + S.sy, k, S.fw, fyp, nullptr);
+        favre_at(P, q, i, j - S.sy, k, S.fw, fym, nullptr);
+        const int kp = min(k + S.sz, n3), km = max(k - S.sz, 1);
+        favre_at(P, q, i, j, kp, S.fw, fzp, nullptr);
+        favre_at(P, q, i, j, km, S.fw, fzm, nullptr);
+        const double cx = 1.0 / (2.0 * S.sx * Lx), cy = 1.0 / (2.0 * S.sy * Ly);
+        const double cz = 1.0 / (S.x3[kp - 1] - S.x3[km - 1]);
+        float *X = S.X + s * 13;
+        // du_a/dx_b, a = u, v, w (fields 1..3), b = x, spanwise, wall-normal; then dT/dx_b
+        for (int m = 0; m < 4; m++) {
+            X[3 * m + 0] = (float)((fxp[m + 1] - fxm[m + 1]) * cx);
+            X[3 * m + 1] = (float)((fyp[m + 1] - fym[m + 1]) * cy);
+            X[3 * m + 2] = (float)((fzp[m + 1] - fzm[m + 1]) * cz);
+        }
+        const double d = fmin(S.x3[k - 1] - S.x3[0], S.x3[n3 - 1] - S.x3[k - 1]);
+        X[12] = (float)(rw * ut * d * (1.0 / P.invRe) / muw);
+        if (S.T) {
+            const double r = f0[0], u = f0[1], v = f0[2], w = f0[3], T = f0[4];
+            float *Tg = S.T + s * 9;
+            Tg[0] = (float)(prod[0] - r * u * u);
+            Tg[1] = (float)(prod[1] - r * v * v);
+            Tg[2] = (float)(prod[2] - r * w * w);
+            Tg[3] = (float)(prod[3] - r * u * v);
+            Tg[4] = (float)(prod[4] - r * u * w);
+            Tg[5] = (float)(prod[5] - r * v * w);
+            Tg[6] = (float)(prod[6] - r * u * T);
+            Tg[7] = (float)(prod[7] - r * v * T);
+            Tg[8] = (float)(prod[8] - r * w * T);
+        }
+    }
+}
+
+// Closure source at the interior points from the subgrid fluxes Y [n][9]
+// (n = (n1-2)(n2-2)(n3-2), index ((k-2)(n2-2) + (j-2))(n1-2) + i-2; zero on
+// the walls): S(rho u_a) = -d tau_ab / dx_b, S(rho E) = -gama d q_b / dx_b
+// (the enthalpy flux gama*rho*u*T of the reference's energy equation).
+__global__ void k_sgs_div(const KParams P, const float *Y, double gama, double *S)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3, m1 = n1 - 2, m2 = n2 - 2;
+    const long long n = (long long)m1 * m2 * (n3 - 2);
+    auto at = [&](int i, int j, int k, int c) -> double {
+        if (k <= 1 || k >= n3) return 0.0;
+        i = wrap_any(i, n1);
+        j = wrap_any(j, n2);
+        return (double)Y[((((long long)(k - 2) * m2) + (j - 2)) * m1 + (i - 2)) * 9 + c];
+    };
+    // flux component of (row a, direction b): tau_ab, or q_b for the energy row
+    auto comp = [](int a, int b) {
+        const int t[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+        return a < 3 ? t[a][b] : 6 + b;
+    };
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const int i = 2 + (int)(s % m1), j = 2 + (int)((s / m1) % m2), k = 2 + (int)(s / ((long long)m1 * m2));
+        const double cz = P.czh[k];
+        for (int a = 0; a < 4; a++) {
+            const double d = (at(i + 1, j, k, comp(a, 0)) - at(i - 1, j, k, comp(a, 0))) * P.hdx +
+                             (at(i, j + 1, k, comp(a, 1)) - at(i, j - 1, k, comp(a, 1))) * P.hdy +
+                             (at(i, j, k + 1, comp(a, 2)) - at(i, j, k - 1, comp(a, 2))) * cz;
+            S[(size_t)a * n + s] = a < 3 ? -d : -gama * d;
+        }
+    }
+}
+
+// q_out += cdt * S at every stored point of the interior planes (periodic
+// duplicates and ghosts take their image's source)
+__global__ void k_sgs_apply(const KParams P, double *qo, const double *S, double cdt)
+{
+    const int n1 = P.n1, n2 = P.n2, n3 = P.n3, m1 = n1 - 2, m2 = n2 - 2;
+    const long long n = (long long)m1 * m2 * (n3 - 2);
+    const long long tot = (long long)(n1 + 2) * (n2 + 2) * (n3 - 2);
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < tot; s += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % (n1 + 2)), j = (int)((s / (n1 + 2)) % (n2 + 2)), k = 2 + (int)(s / ((long long)(n1 + 2) * (n2 + 2)));
+        const int iu = wrap_any(i, n1), ju = wrap_any(j, n2);
+        const long long src = (((long long)(k - 2) * m2) + (ju - 2)) * m1 + (iu - 2);
+        const long long o = (long long)k * P.plane + (long long)j * P.px + i;
+        // S rows: rho*u, rho*v, rho*w, rho*E (state variables 1..4)
+#pragma unroll
+        for (int a = 0; a < 4; a++) qo[o + (a + 1) * P.vol] += cdt * S[(size_t)a * n + src];
+    }
+}
+
 // start of a step in a graph replay: step += 1, time += dt (the host's order)
 __global__ void k_clock_advance(DevClock *clk, double dt)
 {

@@ -4,6 +4,7 @@
 // written inside chan_upload, chan_download and chan_stats.  All work is
 // queued on one CUDA stream per context.
 #include "chanrhs.h"
+#include "chan_internal.h"
 #include "chan_kernels.cuh"
 
 #include <algorithm>
@@ -111,6 +112,13 @@ struct chan_ctx {
     // changes them, so that an ensemble knows when its captured graph is stale
     chan::DevClock *dclk = nullptr;
     long long epoch = 0;
+    // learned subgrid closure (chan_set_closure): features, fluxes, source
+    chan_closure *cl = nullptr;
+    bool closure_on = false;
+    double *dx3 = nullptr;                 // x3 on the device (allocated on first use)
+    float *sgsX = nullptr, *sgsY = nullptr;
+    double *sgsS = nullptr;
+    int *sgsflag = nullptr;
 };
 
 namespace {
@@ -263,6 +271,39 @@ int set_launch(chan_ctx *c, int tile, int nchunks)
     return CHAN_OK;
 }
 
+// device copy of x3 (closure features need the wall-normal coordinates)
+int ensure_dx3(chan_ctx *c)
+{
+    if (c->dx3) return CHAN_OK;
+    CK(c, cudaMalloc((void **)&c->dx3, (size_t)c->n3 * sizeof(double)));
+    CK(c, cudaMemcpy(c->dx3, c->hx3.data(), (size_t)c->n3 * sizeof(double), cudaMemcpyHostToDevice));
+    c->dev_bytes += (size_t)c->n3 * sizeof(double);
+    return CHAN_OK;
+}
+
+// features of the stage input at every interior point, the closure MLP, and
+// the source it gives (applied to the stage output after the stage kernel)
+int closure_source(chan_ctx *c)
+{
+    chan::SgsSampling S{};
+    S.sx = S.sy = S.sz = 1;
+    S.fw = 0;
+    S.i0 = 2; S.ni = c->n1 - 2;
+    S.j0 = 2; S.nj = c->n2 - 2;
+    S.k0 = 2; S.nk = c->n3 - 2;
+    S.x3 = c->dx3;
+    S.X = c->sgsX;
+    S.T = nullptr;
+    const long long n = (long long)S.ni * S.nj * S.nk;
+    chan::k_sgs_sample<<<1184, 128, 0, c->stream>>>(c->kp, (const double *)c->kp.qin, S);
+    CK(c, cudaGetLastError());
+    int r = chan_internal_infer(c->cl, c->sgsX, c->sgsY, n, c->stream, c->sgsflag);
+    if (r) { c->err = "closure inference"; return r; }
+    chan::k_sgs_div<<<1184, 256, 0, c->stream>>>(c->kp, c->sgsY, c->p.gama, c->sgsS);
+    CK(c, cudaGetLastError());
+    return CHAN_OK;
+}
+
 int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
 {
     set_stage(c, iter);
@@ -271,12 +312,20 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
     c->kp.check = check ? 1 : 0;
     c->kp.step = step;
     const bool last = iter == c->nstage;
+    if (c->closure_on) {
+        int r = closure_source(c);
+        if (r) return r;
+    }
     {
         ProfScope ps(c, 0);
         const StageSet &ss = kStageSets[c->tile];
         dim3 grid(c->ntx, c->nty, c->nchunks), block(ss.ti, ss.tj);
         const int v = !c->mixed ? 0 : (iter == 1 ? 1 : (last ? 3 : 2));
         ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(c->kp);
+    }
+    if (c->closure_on) {
+        chan::k_sgs_apply<<<1184, 256, 0, c->stream>>>(c->kp, (double *)c->kp.qout, c->sgsS, c->kp.rk_cdt);
+        CK(c, cudaGetLastError());
     }
     CK(c, cudaGetLastError());
     {
@@ -975,6 +1024,44 @@ int chan_set_buoyancy(chan_ctx *c, double Ri, double Tref)
     return CHAN_OK;
 }
 
+int chan_set_closure(chan_ctx *c, chan_closure *m, int32_t on)
+{
+    if (!c) return CHAN_EINVAL;
+    if (on && !m) return CHAN_EINVAL;
+    if (on && c->mixed) { c->err = "the closure runs on plain FP64 contexts"; return CHAN_EINVAL; }
+    CK(c, cudaSetDevice(c->dev));
+    if (on && chan_internal_closure_device(m) != c->dev) { c->err = "closure on another device"; return CHAN_EINVAL; }
+    if (on && !c->sgsX) {
+        const long long n = (long long)(c->n1 - 2) * (c->n2 - 2) * (c->n3 - 2);
+        int r = ensure_dx3(c);
+        if (r) return r;
+        CK(c, cudaMalloc((void **)&c->sgsX, (size_t)n * chan::kSgsIn * sizeof(float)));
+        CK(c, cudaMalloc((void **)&c->sgsY, (size_t)n * chan::kSgsOut * sizeof(float)));
+        CK(c, cudaMalloc((void **)&c->sgsS, (size_t)n * 4 * sizeof(double)));
+        CK(c, cudaMalloc((void **)&c->sgsflag, sizeof(int)));
+        CK(c, cudaMemset(c->sgsflag, 0, sizeof(int)));
+        c->dev_bytes += (size_t)n * ((chan::kSgsIn + chan::kSgsOut) * sizeof(float) + 4 * sizeof(double)) + sizeof(int);
+    }
+    c->cl = on ? m : nullptr;
+    c->closure_on = on != 0;
+    c->epoch++;
+    return CHAN_OK;
+}
+
+int chan_closure_flag(chan_ctx *c, int32_t *flag, int32_t reset)
+{
+    if (!c || !flag) return CHAN_EINVAL;
+    *flag = 0;
+    if (!c->sgsflag) return CHAN_OK;
+    CK(c, cudaSetDevice(c->dev));
+    CK(c, cudaMemcpyAsync(c->h_status, c->sgsflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    *flag = *(const int *)c->h_status;
+    if (reset) CK(c, cudaMemsetAsync(c->sgsflag, 0, sizeof(int), c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return CHAN_OK;
+}
+
 int chan_set_launch(chan_ctx *c, int32_t tile, int32_t nchunks)
 {
     if (!c) return CHAN_EINVAL;
@@ -1318,6 +1405,11 @@ void chan_free(chan_ctx *c)
     if (c->diag_part) cudaFree(c->diag_part);
     if (c->diag_x3) cudaFree(c->diag_x3);
     if (c->dq) cudaFree(c->dq);
+    if (c->dx3) cudaFree(c->dx3);
+    if (c->sgsX) cudaFree(c->sgsX);
+    if (c->sgsY) cudaFree(c->sgsY);
+    if (c->sgsS) cudaFree(c->sgsS);
+    if (c->sgsflag) cudaFree(c->sgsflag);
     if (c->dxyz) cudaFree(c->dxyz);
     if (c->status) cudaFree(c->status);
     if (c->h_status) cudaFreeHost(c->h_status);
@@ -1718,3 +1810,33 @@ void chan_ensemble_free(chan_ensemble *e)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// closure training samples from a context's current state (chan_internal.h)
+int chan_internal_sample(chan_ctx *c, float *X, float *T, long long capacity, int sx, int sy, int sz, int fw,
+                         long long *added)
+{
+    *added = 0;
+    if (!c || !X || !T || sx < 1 || sy < 1 || sz < 1 || fw < 0 || fw % 2) return CHAN_EINVAL;
+    if (!c->uploaded) return CHAN_ESTATE;
+    CK(c, cudaSetDevice(c->dev));
+    int r = ensure_dx3(c);
+    if (r) return r;
+    chan::SgsSampling S{};
+    S.sx = sx; S.sy = sy; S.sz = sz; S.fw = fw;
+    S.i0 = 2; S.ni = (c->n1 - 3) / sx + 1;
+    S.j0 = 2; S.nj = (c->n2 - 3) / sy + 1;
+    S.k0 = 1 + sz; S.nk = (c->n3 - 1) / sz - 1;
+    if (S.nk < 1) return CHAN_EINVAL;
+    const long long n = (long long)S.ni * S.nj * S.nk;
+    if (n > capacity) { c->err = "closure dataset full"; return CHAN_EINVAL; }
+    S.x3 = c->dx3;
+    S.X = X;
+    S.T = T;
+    // the state after whole steps: q[cur] in double
+    chan::k_sgs_sample<<<1184, 128, 0, c->stream>>>(c->kp, c->q[c->cur], S);
+    CK(c, cudaGetLastError());
+    CK(c, cudaStreamSynchronize(c->stream));
+    *added = n;
+    return CHAN_OK;
+}

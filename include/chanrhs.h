@@ -346,6 +346,70 @@ int chan_q_criterion(const int32_t *nP, const double *u, const double *v, const 
  * memory checker in tests; the reference has no counterpart. */
 int chan_debug_canaries(chan_ctx *c, int64_t *corrupted);
 
+/* ------------------------------------------------------------------------
+ * Learned subgrid closure (no reference counterpart: the reference resolves
+ * every scale).  A 13 -> 64 -> 64 -> 9 MLP with GELU activations, BF16
+ * weights and activations and F32 accumulation on the tensor cores (tcgen05),
+ * F32 master weights trained with Adam on the device.
+ *   inputs : du_a/dx_b (a = u, v, w; b = x, spanwise, wall-normal; 9), dT/dx_b
+ *            (3) and y+ = rho_w u_tau d Re / mu_w, d the distance to the
+ *            nearer wall;
+ *   outputs: the Favre subgrid fluxes tau_ab = bar(rho u_a u_b) - bar(rho)
+ *            u~_a u~_b (uu, vv, ww, uv, uw, vw) and q_b = bar(rho u_b T) -
+ *            bar(rho) u~_b T~ (u, v, w).
+ * Both are normalised by a per-column mean and standard deviation
+ * (norm[44] = input means[13], input sds[13], output means[9], output sds[9]).
+ * Parameters: W1[64][13] b1[64] W2[64][64] b2[64] W3[9][64] b3[9]
+ * (chan_closure_nparams() floats). */
+typedef struct chan_closure chan_closure;
+/* capacity: samples the device dataset holds (13 + 9 floats each) */
+int chan_closure_create(int32_t device, int64_t capacity, chan_closure **out);
+/* Append samples of a DNS context's current state: the Favre box filter of
+ * width fw (even) in x and spanwise, sample points every (sx, sy, sz) grid
+ * points away from the walls, gradients by central differences at those
+ * strides (the coarse grid the closure runs on). */
+int chan_closure_sample(chan_closure *m, chan_ctx *dns, int32_t sx, int32_t sy, int32_t sz, int32_t fw,
+                        int64_t *added);
+/* append host samples X[n][13], T[n][9] (a saved dataset, or synthetic data) */
+int chan_closure_add_data(chan_closure *m, const float *X, const float *T, int64_t n);
+int chan_closure_count(chan_closure *m, int64_t *count);
+int chan_closure_get_data(chan_closure *m, int64_t first, int64_t n, float *X, float *T);
+/* mean / standard deviation of the dataset's columns -> normalisation */
+int chan_closure_fit_normalization(chan_closure *m, float *norm_out);
+int chan_closure_set_normalization(chan_closure *m, const float *norm);
+int chan_closure_get_normalization(chan_closure *m, float *norm);
+int chan_closure_nparams(void);
+/* Glorot-uniform weights from a seeded generator, zero biases */
+int chan_closure_init(chan_closure *m, uint64_t seed);
+int chan_closure_set_params(chan_closure *m, const float *params);
+int chan_closure_get_params(chan_closure *m, float *params);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) on the mean squared error of the
+ * normalised outputs, batches of `batch` samples (a multiple of 128) in a
+ * seeded order per epoch; losses[epochs] receives each epoch's mean loss. */
+int chan_closure_train(chan_closure *m, int32_t epochs, int32_t batch, double lr, uint64_t seed, double *losses);
+/* loss sum and parameter gradients (chan_closure_nparams floats) of the mean
+ * squared error over one host batch, as one training step computes them */
+int chan_closure_grad(chan_closure *m, const float *X, const float *T, int64_t n, float *grads, double *loss_sum);
+/* outputs in physical units for host inputs */
+int chan_closure_infer(chan_closure *m, const float *X, int64_t n, float *Y);
+const char *chan_closure_last_error(chan_closure *m);
+void chan_closure_free(chan_closure *m);
+
+/* Run a context with the closure (on = 1) or without it (on = 0).  Every
+ * stage then evaluates the features of its input state at the interior
+ * points (central differences on the context's own grid), the MLP, and adds
+ * cdt * S to the stage output, S(rho u_a) = -d tau_ab / dx_b and
+ * S(rho E) = -gama d q_b / dx_b (zero fluxes on the walls).  Plain FP64
+ * contexts only.  chan_closure_flag reports (and optionally resets) whether
+ * a normalised output exceeded 50 in magnitude since the last reset. */
+int chan_set_closure(chan_ctx *c, chan_closure *m, int32_t on);
+int chan_closure_flag(chan_ctx *c, int32_t *flag, int32_t reset);
+
+/* Tensor-core self-test: D[128][N] = A[128][K] * B[N][K]^T with BF16 A and B
+ * (raw bit patterns, row-major) and F32 D, through the same tcgen05 path the
+ * closure MLP uses (K and N multiples of 16 up to 256).  For tests. */
+int chan_selftest_umma(const uint16_t *A, const uint16_t *B, float *D, int32_t K, int32_t N, int32_t device);
+
 /* Free device memory and the context.  NULL is allowed.  A context that is a
  * member of an ensemble is freed after its ensemble. */
 void chan_free(chan_ctx *c);

@@ -157,3 +157,28 @@ def test_oracle_buoyancy_source_is_the_stated_term():
     assert np.max(np.abs(bq)) > 1e-3
     assert np.max(np.abs(dw - cdt * bq)) <= 1e-12 * np.max(np.abs(qa[3][sl])) + 1e-15
     assert np.max(np.abs(dE - cdt * p.ggM * w * bq)) <= 1e-12 * np.max(np.abs(qa[4][sl])) + 1e-15
+
+
+def test_closure_oracle_gradient_matches_finite_differences():
+    """The oracle's MLP backward pass (without its BF16 roundings) is the
+    derivative of its loss: checked by central differences in float64."""
+    from oracle import closure_oracle as C
+    rng = np.random.default_rng(3)
+    params = rng.standard_normal(C.N_PARAM) * 0.3
+    norm = np.concatenate([np.zeros(13), np.ones(13), np.zeros(9), np.ones(9)])
+    X = rng.standard_normal((40, 13))
+    T = rng.standard_normal((40, 9))
+    ident = lambda x: np.asarray(x, dtype=np.float64)   # noqa: E731
+    orig = C.bf16
+    C.bf16 = ident
+    try:
+        loss, g = C.grad(params, norm, X, T)
+        for idx in list(range(0, C.N_PARAM, 97)) + [C.OFF_B1 + 3, C.OFF_B3 + 2, C.OFF_W3 + 5]:
+            e = np.zeros(C.N_PARAM)
+            e[idx] = 1e-6
+            lp, _ = C.grad(params + e, norm, X, T)
+            lm, _ = C.grad(params - e, norm, X, T)
+            fd = (lp - lm) / (2e-6) / (9.0 * 40)
+            assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(g[idx])), (idx, fd, g[idx])
+    finally:
+        C.bf16 = orig
