@@ -165,9 +165,11 @@ class Closure:
             pass
 
 
-def attach(ch: Channel, cl: Closure | None, on: bool = True):
-    """Switch the closure of a coarse context on or off."""
-    r = ch.L.chan_set_closure(ch._h, cl._h if (cl is not None and on) else None, 1 if on else 0)
+def attach(ch: Channel, cl: Closure | None, on: bool = True, every_stage: bool = False):
+    """Switch the closure of a coarse context on or off; by default its source
+    is evaluated once per step (at the first stage) and held for the others."""
+    mode = (2 if every_stage else 1) if on else 0
+    r = ch.L.chan_set_closure(ch._h, cl._h if (cl is not None and on) else None, mode)
     ch._check(r)
     ch._closure = cl if on else None
 

@@ -21,8 +21,9 @@ constexpr int kClIn = 13, kClOut = 9;
 int chan_internal_sample(chan_ctx *c, float *X, float *T, long long capacity, int sx, int sy, int sz, int fw,
                          long long *added);
 
-// MLP inference on device arrays: Y [n][9] in physical units from X [n][13];
-// sets *flag (device) when a normalised output exceeds the closure's limit.
-// Queued on `stream`, not synchronised.
-int chan_internal_infer(chan_closure *m, const float *X, float *Y, long long n, cudaStream_t stream, int *flag);
+// MLP inference on device arrays: Y [n][9] in physical units from X [n][13]
+// (soa: X [13][n] and Y [9][n]); sets *flag (device) when a normalised output
+// exceeds the closure's limit.  Queued on `stream`, not synchronised.
+int chan_internal_infer(chan_closure *m, const float *X, float *Y, long long n, bool soa, cudaStream_t stream,
+                        int *flag);
 int chan_internal_closure_device(chan_closure *m);

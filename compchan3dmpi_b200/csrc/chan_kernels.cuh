@@ -1521,7 +1521,10 @@ constexpr int kSgsIn = 13, kSgsOut = 9;   // closure features and fluxes per poi
 // periodic image of any x or spanwise index on the unique points 2..n-1
 __device__ __forceinline__ int wrap_any(int i, int n)
 {
+    if (i >= 2 && i <= n - 1) return i;
     const int m = n - 2;
+    if (i >= 2 - m && i < 2) return i + m;
+    if (i > n - 1 && i <= n - 1 + m) return i - m;
     int r = (i - 2) % m;
     if (r < 0) r += m;
     return r + 2;
@@ -1539,12 +1542,12 @@ __device__ __forceinline__ void prim_at(const KParams &P, const double *q, int i
         return;
     }
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
-    const double r = q[o];
+    const double r = q[o], ri = 1.0 / r;
     x[0] = r;
-    x[1] = q[P.vol + o] / r;
-    x[2] = q[2 * P.vol + o] / r;
-    x[3] = q[3 * P.vol + o] / r;
-    x[4] = q[4 * P.vol + o] / r - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
+    x[1] = q[P.vol + o] * ri;
+    x[2] = q[2 * P.vol + o] * ri;
+    x[3] = q[3 * P.vol + o] * ri;
+    x[4] = q[4 * P.vol + o] * ri - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
 }
 
 // Favre-filtered (rho, u, v, w, T) at (i, j, k): a box of width fw (even)
@@ -1593,6 +1596,7 @@ struct SgsSampling {
     int i0, ni, j0, nj, k0, nk;  // sample points i0 + sx*a (a < ni), j0 + sy*b, k0 + sz*c
     const double *x3;            // x3(1..nP3) at x3[k-1]
     float *X, *T;                // [n][13], [n][9] (T may be null)
+    bool soa;                    // X as [13][n] instead (the closure run's layout)
 };
 
 // Features (and with T the filtered subgrid fluxes) at every sample point.
@@ -1622,15 +1626,16 @@ __global__ void k_sgs_sample(const KParams P, const double *q, const SgsSampling
         favre_at(P, q, i, j, km, S.fw, fzm, nullptr);
         const double cx = 1.0 / (2.0 * S.sx * Lx), cy = 1.0 / (2.0 * S.sy * Ly);
         const double cz = 1.0 / (S.x3[kp - 1] - S.x3[km - 1]);
-        float *X = S.X + s * 13;
+        float *X = S.soa ? S.X + s : S.X + s * 13;
+        const long long xc = S.soa ? n : 1;
         // du_a/dx_b, a = u, v, w (fields 1..3), b = x, spanwise, wall-normal; then dT/dx_b
         for (int m = 0; m < 4; m++) {
-            X[3 * m + 0] = (float)((fxp[m + 1] - fxm[m + 1]) * cx);
-            X[3 * m + 1] = (float)((fyp[m + 1] - fym[m + 1]) * cy);
-            X[3 * m + 2] = (float)((fzp[m + 1] - fzm[m + 1]) * cz);
+            X[(3 * m + 0) * xc] = (float)((fxp[m + 1] - fxm[m + 1]) * cx);
+            X[(3 * m + 1) * xc] = (float)((fyp[m + 1] - fym[m + 1]) * cy);
+            X[(3 * m + 2) * xc] = (float)((fzp[m + 1] - fzm[m + 1]) * cz);
         }
         const double d = fmin(S.x3[k - 1] - S.x3[0], S.x3[n3 - 1] - S.x3[k - 1]);
-        X[12] = (float)(rw * ut * d * (1.0 / P.invRe) / muw);
+        X[12 * xc] = (float)(rw * ut * d * (1.0 / P.invRe) / muw);
         if (S.T) {
             const double r = f0[0], u = f0[1], v = f0[2], w = f0[3], T = f0[4];
             float *Tg = S.T + s * 9;
@@ -1647,7 +1652,7 @@ __global__ void k_sgs_sample(const KParams P, const double *q, const SgsSampling
     }
 }
 
-// Closure source at the interior points from the subgrid fluxes Y [n][9]
+// Closure source at the interior points from the subgrid fluxes Y [9][n]
 // (n = (n1-2)(n2-2)(n3-2), index ((k-2)(n2-2) + (j-2))(n1-2) + i-2; zero on
 // the walls): S(rho u_a) = -d tau_ab / dx_b, S(rho E) = -gama d q_b / dx_b
 // (the enthalpy flux gama*rho*u*T of the reference's energy equation).
@@ -1659,7 +1664,7 @@ __global__ void k_sgs_div(const KParams P, const float *Y, double gama, double *
         if (k <= 1 || k >= n3) return 0.0;
         i = wrap_any(i, n1);
         j = wrap_any(j, n2);
-        return (double)Y[((((long long)(k - 2) * m2) + (j - 2)) * m1 + (i - 2)) * 9 + c];
+        return (double)Y[(long long)c * n + (((long long)(k - 2) * m2) + (j - 2)) * m1 + (i - 2)];
     };
     // flux component of (row a, direction b): tau_ab, or q_b for the energy row
     auto comp = [](int a, int b) {

@@ -115,6 +115,8 @@ struct chan_ctx {
     // learned subgrid closure (chan_set_closure): features, fluxes, source
     chan_closure *cl = nullptr;
     bool closure_on = false;
+    bool closure_every_stage = false;   // else the source of a step's first stage is held for its other stages
+    bool sgs_valid = false;             // sgsS holds a source for the current step
     double *dx3 = nullptr;                 // x3 on the device (allocated on first use)
     float *sgsX = nullptr, *sgsY = nullptr;
     double *sgsS = nullptr;
@@ -294,10 +296,11 @@ int closure_source(chan_ctx *c)
     S.x3 = c->dx3;
     S.X = c->sgsX;
     S.T = nullptr;
+    S.soa = true;
     const long long n = (long long)S.ni * S.nj * S.nk;
     chan::k_sgs_sample<<<1184, 128, 0, c->stream>>>(c->kp, (const double *)c->kp.qin, S);
     CK(c, cudaGetLastError());
-    int r = chan_internal_infer(c->cl, c->sgsX, c->sgsY, n, c->stream, c->sgsflag);
+    int r = chan_internal_infer(c->cl, c->sgsX, c->sgsY, n, true, c->stream, c->sgsflag);
     if (r) { c->err = "closure inference"; return r; }
     chan::k_sgs_div<<<1184, 256, 0, c->stream>>>(c->kp, c->sgsY, c->p.gama, c->sgsS);
     CK(c, cudaGetLastError());
@@ -312,9 +315,10 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
     c->kp.check = check ? 1 : 0;
     c->kp.step = step;
     const bool last = iter == c->nstage;
-    if (c->closure_on) {
+    if (c->closure_on && (iter == 1 || c->closure_every_stage || !c->sgs_valid)) {
         int r = closure_source(c);
         if (r) return r;
+        c->sgs_valid = true;
     }
     {
         ProfScope ps(c, 0);
@@ -751,6 +755,7 @@ int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time)
     c->sync_time = time;
     c->cur = 0;
     c->uploaded = true;
+    c->sgs_valid = false;
     return CHAN_OK;
 }
 
@@ -1010,6 +1015,7 @@ int chan_checkpoint_read(chan_ctx *c, const char *path)
     c->epoch++;
     c->cur = 0;
     c->uploaded = true;
+    c->sgs_valid = false;
     return CHAN_OK;
 }
 
@@ -1027,7 +1033,7 @@ int chan_set_buoyancy(chan_ctx *c, double Ri, double Tref)
 int chan_set_closure(chan_ctx *c, chan_closure *m, int32_t on)
 {
     if (!c) return CHAN_EINVAL;
-    if (on && !m) return CHAN_EINVAL;
+    if (on < 0 || on > 2 || (on && !m)) return CHAN_EINVAL;
     if (on && c->mixed) { c->err = "the closure runs on plain FP64 contexts"; return CHAN_EINVAL; }
     CK(c, cudaSetDevice(c->dev));
     if (on && chan_internal_closure_device(m) != c->dev) { c->err = "closure on another device"; return CHAN_EINVAL; }
@@ -1044,6 +1050,8 @@ int chan_set_closure(chan_ctx *c, chan_closure *m, int32_t on)
     }
     c->cl = on ? m : nullptr;
     c->closure_on = on != 0;
+    c->closure_every_stage = on == 2;
+    c->sgs_valid = false;
     c->epoch++;
     return CHAN_OK;
 }

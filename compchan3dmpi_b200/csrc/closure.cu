@@ -83,14 +83,15 @@ struct WImages {
 struct MlpParams {
     const unsigned char *wimg;   // WImages::bytes of BF16 images
     const float *b1, *b2, *b3;   // biases (64, 64, 9)
-    const float *X;              // [n][13] inputs (raw)
+    const float *X;              // inputs (raw): X[row * xr + f * xc]
     const float *T;              // [n][9] targets (raw), training only
     const float *xmu, *xsd;      // input normalisation (13 each)
     const float *ymu, *ysd;      // output normalisation (9 each)
     long long n;                 // samples
     long long perm_a, perm_b;    // sample of batch row r: (perm_a * (row0 + r) + perm_b) mod n
     long long row0, rows;        // batch rows [row0, row0 + rows)
-    float *Y;                    // [rows][9] outputs (raw units), inference only
+    float *Y;                    // outputs (raw units), inference only: Y[row * yr + o * yc]
+    long long xr, xc, yr, yc;    // element strides of X and Y (rows, columns)
     float *gW1, *gW2, *gW3, *gb1, *gb2, *gb3;   // gradient sums (training)
     float *loss;                 // sum of squared normalised errors (training)
     float inv_count;             // 2 / (9 * rows): d loss / d y factor
@@ -99,10 +100,24 @@ struct MlpParams {
     int *err;
 };
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), on
+// the hardware tanh approximation (tanh.approx.f32), and its derivative
+__device__ __forceinline__ float tanh_hw(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluA = 0.7978845608028654f, kGeluB = 0.044715f;
+__device__ __forceinline__ float gelu(float z)
+{
+    const float t = tanh_hw(kGeluA * (z + kGeluB * z * z * z));
+    return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_d(float z)
 {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * (0.39894228040143268f * expf(-0.5f * z * z));
+    const float t = tanh_hw(kGeluA * (z + kGeluB * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluA * (1.0f + 3.0f * kGeluB * z * z);
 }
 
 __device__ __forceinline__ float warp_sum(float v)
@@ -142,30 +157,51 @@ struct MlpSmem {
     static constexpr int bytes = fl + (64 + 64 + 16 + 64 + 64 + 16 + 4) * 4;
 };
 
-// tensor-memory columns
-constexpr int cZ1 = 0, cZ2 = 64, cY = 128, cdH2 = 192, cdH1 = 256, cdW3 = 320, cdW2 = 384, cdW1 = 448;
+// Shared memory of the inference-only kernel: the forward weight images, X, H1, H2
+struct InferSmem {
+    static constexpr int wbytes = WImages::w2t;                      // W1, W2, W3 images
+    static constexpr int x = wbytes;
+    static constexpr int h1 = x + kTile * kInP * 2;
+    static constexpr int h2 = h1 + kTile * kHid * 2;
+    static constexpr int fl = h2 + kTile * kHid * 2;
+    static constexpr int bytes = fl + (64 + 64 + 16 + 64 + 64 + 16 + 4) * 4;
+};
+
+// tensor-memory columns: training holds all 512 (one CTA per SM); inference
+// needs Z1, Z2 and Y, with Y over Z1's columns (128, four CTAs per SM)
+constexpr int cZ1 = 0, cZ2 = 64, cdH2 = 192, cdH1 = 256, cdW3 = 320, cdW2 = 384, cdW1 = 448;
+template <bool TRAIN>
+struct MlpCfg {
+    static constexpr int cY = TRAIN ? 128 : 0, tmem = TRAIN ? 512 : 128, minb = TRAIN ? 1 : 4;
+    static constexpr int wbytes = TRAIN ? WImages::bytes : InferSmem::wbytes;
+    static constexpr int x = TRAIN ? MlpSmem::x : InferSmem::x, h1 = TRAIN ? MlpSmem::h1 : InferSmem::h1,
+                         h2 = TRAIN ? MlpSmem::h2 : InferSmem::h2, fl = TRAIN ? MlpSmem::fl : InferSmem::fl,
+                         bytes = TRAIN ? MlpSmem::bytes : InferSmem::bytes;
+};
 
 // Forward (and for TRAIN the backward) pass over the batch rows, 128 per
 // tile, tiles strided over the grid; one CTA of 128 threads per SM (the CTA
 // holds all 512 tensor-memory columns).  Thread t owns row t of each tile.
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P)
+__global__ void __launch_bounds__(128, MlpCfg<TRAIN>::minb) k_mlp(const MlpParams P)
 {
+    using G = MlpCfg<TRAIN>;
+    constexpr int cY = G::cY;
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tbase;
     const int tid = threadIdx.x, warp = tid >> 5;
-    float *fb1 = (float *)(sm + MlpSmem::fl), *fb2 = fb1 + 64, *fb3 = fb2 + 64;
+    float *fb1 = (float *)(sm + G::fl), *fb2 = fb1 + 64, *fb3 = fb2 + 64;
     float *db1 = fb3 + 16, *db2 = db1 + 64, *db3 = db2 + 64, *sloss = db3 + 16;
     {   // weight images and biases
         const uint4 *src = (const uint4 *)P.wimg;
         uint4 *dst = (uint4 *)(sm + MlpSmem::w);
-        for (int e = tid; e < WImages::bytes / 16; e += 128) dst[e] = src[e];
+        for (int e = tid; e < G::wbytes / 16; e += 128) dst[e] = src[e];
         if (tid < 64) { fb1[tid] = P.b1[tid]; fb2[tid] = P.b2[tid]; db1[tid] = 0.f; db2[tid] = 0.f; }
         if (tid < 16) { fb3[tid] = tid < kOut ? P.b3[tid] : 0.f; db3[tid] = 0.f; }
         if (tid == 0) sloss[0] = 0.f;
     }
-    if (warp == 0) umma::tmem_alloc(&tbase, 512);
+    if (warp == 0) umma::tmem_alloc(&tbase, G::tmem);
     if (tid == 0) umma::mbar_init(&mbar, 1);
     umma::fence_async_smem();
     umma::fence_before_sync();
@@ -173,7 +209,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P)
     umma::fence_after_sync();
     const uint32_t tb = tbase;
     unsigned char *sW = sm + MlpSmem::w;
-    unsigned char *sX = sm + MlpSmem::x, *sH1 = sm + MlpSmem::h1, *sH2 = sm + MlpSmem::h2;
+    unsigned char *sX = sm + G::x, *sH1 = sm + G::h1, *sH2 = sm + G::h2;
     unsigned char *sdY = sm + MlpSmem::dy, *sdZ2 = sm + MlpSmem::dz2;
     unsigned char *sXt = sm + MlpSmem::xt, *sH1t = sm + MlpSmem::h1t, *sH2t = sm + MlpSmem::h2t;
     unsigned char *sGt = sm + MlpSmem::gt;
@@ -207,7 +243,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P)
         float xin[kInP], tgt[kOut];
 #pragma unroll
         for (int f = 0; f < kInP; f++)
-            xin[f] = (live && f < kIn) ? (P.X[sample * kIn + f] - P.xmu[f]) / P.xsd[f] : 0.f;
+            xin[f] = (live && f < kIn) ? (P.X[sample * P.xr + f * P.xc] - P.xmu[f]) / P.xsd[f] : 0.f;
         if (TRAIN) {
 #pragma unroll
             for (int o = 0; o < kOut; o++) tgt[o] = live ? (P.T[sample * kOut + o] - P.ymu[o]) / P.ysd[o] : 0.f;
@@ -261,7 +297,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P)
 #pragma unroll
                 for (int o = 0; o < kOut; o++) {
                     big = big || !(fabsf(y[o]) <= P.out_limit);
-                    P.Y[row * kOut + o] = y[o] * P.ysd[o] + P.ymu[o];
+                    P.Y[row * P.yr + o * P.yc] = y[o] * P.ysd[o] + P.ymu[o];
                 }
                 if (big && P.flag) atomicOr(P.flag, 1);
             }
@@ -371,7 +407,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P)
         }
         __syncthreads();
     }
-    if (warp == 0) umma::tmem_free(tb, 512);
+    if (warp == 0) umma::tmem_free(tb, G::tmem);
 }
 
 // Adam on the F32 master parameters, then the BF16 weight images.
@@ -497,6 +533,7 @@ MlpParams base_params(chan_closure *m)
     P.err = m->err;
     P.out_limit = m->out_limit;
     P.perm_a = 1; P.perm_b = 0;
+    P.xr = kIn; P.xc = 1; P.yr = kOut; P.yc = 1;
     return P;
 }
 
@@ -510,10 +547,11 @@ int refresh_images(chan_closure *m)
 int launch_mlp(chan_closure *m, const MlpParams &P, bool train, cudaStream_t st)
 {
     const long long ntiles = (P.rows + kTile - 1) / kTile;
-    const int grid = (int)(ntiles < m->sms ? ntiles : m->sms);
+    const long long slots = (long long)m->sms * (train ? MlpCfg<true>::minb : MlpCfg<false>::minb);
+    const int grid = (int)(ntiles < slots ? ntiles : slots);
     if (grid < 1) return CHAN_OK;
-    if (train) k_mlp<true><<<grid, 128, MlpSmem::bytes, st>>>(P);
-    else k_mlp<false><<<grid, 128, MlpSmem::bytes, st>>>(P);
+    if (train) k_mlp<true><<<grid, 128, MlpCfg<true>::bytes, st>>>(P);
+    else k_mlp<false><<<grid, 128, MlpCfg<false>::bytes, st>>>(P);
     CLK(m, cudaGetLastError());
     return CHAN_OK;
 }
@@ -529,10 +567,12 @@ int check_err(chan_closure *m)
 
 }  // namespace
 
-int chan_internal_infer(chan_closure *m, const float *X, float *Y, long long n, cudaStream_t stream, int *flag)
+int chan_internal_infer(chan_closure *m, const float *X, float *Y, long long n, bool soa, cudaStream_t stream,
+                        int *flag)
 {
     MlpParams P = base_params(m);
     P.X = X; P.Y = Y; P.n = n; P.rows = n; P.row0 = 0; P.flag = flag;
+    if (soa) { P.xr = 1; P.xc = n; P.yr = 1; P.yc = n; }
     return launch_mlp(m, P, false, stream);
 }
 
@@ -596,7 +636,7 @@ int chan_closure_create(int32_t device, int64_t capacity, chan_closure **out)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpSmem::bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpSmem::bytes);
+        e = cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpCfg<false>::bytes);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         g_cl_error = std::string("chan_closure_create: ") + cudaGetErrorString(e);
@@ -813,7 +853,7 @@ int chan_closure_infer(chan_closure *m, const float *X, int64_t n, float *Y)
     CLK(m, cudaMalloc((void **)&dY, (size_t)n * kOut * sizeof(float)));
     CLK(m, cudaMemcpy(dX, X, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice));
     CLK(m, cudaMemsetAsync(m->err, 0, sizeof(int), m->stream));
-    int r = chan_internal_infer(m, dX, dY, n, m->stream, nullptr);
+    int r = chan_internal_infer(m, dX, dY, n, false, m->stream, nullptr);
     if (!r) r = check_err(m);
     if (!r) CLK(m, cudaMemcpy(Y, dY, (size_t)n * kOut * sizeof(float), cudaMemcpyDeviceToHost));
     cudaFree(dX);

@@ -395,12 +395,14 @@ int chan_closure_infer(chan_closure *m, const float *X, int64_t n, float *Y);
 const char *chan_closure_last_error(chan_closure *m);
 void chan_closure_free(chan_closure *m);
 
-/* Run a context with the closure (on = 1) or without it (on = 0).  Every
- * stage then evaluates the features of its input state at the interior
- * points (central differences on the context's own grid), the MLP, and adds
- * cdt * S to the stage output, S(rho u_a) = -d tau_ab / dx_b and
- * S(rho E) = -gama d q_b / dx_b (zero fluxes on the walls).  Plain FP64
- * contexts only.  chan_closure_flag reports (and optionally resets) whether
+/* Run a context with the closure (on = 1 or 2) or without it (on = 0).
+ * The closure evaluates the features of a stage's input state at the
+ * interior points (central differences on the context's own grid), the MLP,
+ * and the source S(rho u_a) = -d tau_ab / dx_b, S(rho E) = -gama d q_b / dx_b
+ * (zero fluxes on the walls); every stage adds cdt * S to its output.  With
+ * on = 1 the source of a step's first stage is held for its other stages
+ * (the subgrid term advanced by forward Euler, one evaluation per step); with
+ * on = 2 every stage evaluates it.  Plain FP64 contexts only.  chan_closure_flag reports (and optionally resets) whether
  * a normalised output exceeded 50 in magnitude since the last reset. */
 int chan_set_closure(chan_ctx *c, chan_closure *m, int32_t on);
 int chan_closure_flag(chan_ctx *c, int32_t *flag, int32_t reset);

@@ -8,7 +8,7 @@ library's closure kernels compute, so the tests can check them:
   features (velocity and temperature gradients at the sample strides, y+)
   and the 9 subgrid fluxes, from a primitive field var[7, nP3, nP2, nP1]
   (rho, u, v, w, E, T, p) as chan_download returns it;
-* ``forward`` / ``grad``: the 13 -> 64 -> 64 -> 9 GELU MLP with the BF16
+* ``forward`` / ``grad``: the 13 -> 64 -> 64 -> 9 MLP (tanh-form GELU) with the BF16
   rounding the tensor-core path applies (inputs, hidden activations, output
   and hidden gradients rounded to BF16 before each product; products and
   sums exact here, F32 on the device);
@@ -45,19 +45,17 @@ def unpack(params):
             p[OFF_B2:OFF_W3], p[OFF_W3:OFF_B3].reshape(9, 64), p[OFF_B3:N_PARAM])
 
 
-try:
-    from scipy.special import erf as _erf
-except ImportError:   # pragma: no cover
-    def _erf(x):
-        return np.vectorize(math.erf)(x)
+GELU_A, GELU_B = math.sqrt(2.0 / math.pi), 0.044715
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_A * (z + GELU_B * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(GELU_A * (z + GELU_B * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_A * (1.0 + 3.0 * GELU_B * z * z)
 
 
 def _norm(norm):

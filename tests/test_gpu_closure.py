@@ -184,3 +184,25 @@ def test_divergent_closure_falls_back_to_the_plain_method(tmp_path):
     h.init_sol_v(var)
     h.step(12)
     assert np.array_equal(g.download(), h.download())
+
+
+def test_closure_once_per_step_and_every_stage():
+    """Stage 1 is the same in both modes; over whole steps the two differ only
+    by holding the first stage's source (both stay finite and close)."""
+    p, x3, jac, inv, var = _dns_case()
+    cl, params, norm = _random_closure(seed=21, scale=0.3, ysd=0.01)
+    a = Channel(p, x3, jac, inv)
+    b = Channel(p, x3, jac, inv)
+    attach(a, cl, True)
+    attach(b, cl, True, every_stage=True)
+    for ch in (a, b):
+        ch.init_sol_v(var)
+        ch.stage(1)
+    assert np.array_equal(a.download(), b.download())
+    for ch in (a, b):
+        ch.init_sol_v(var)
+        ch.step(5)
+    va, vb = a.download(), b.download()
+    assert np.all(np.isfinite(va)) and np.all(np.isfinite(vb))
+    assert not np.array_equal(va, vb)
+    assert np.max(np.abs(va - vb)) < 5e-2 * np.max(np.abs(vb))
