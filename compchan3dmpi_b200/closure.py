@@ -367,8 +367,30 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     return out, params, norm
 
 
+def synthetic_train(n: int, epochs: int, batch: int = 65536, seed: int = 4):
+    """Training throughput on a synthetic dataset of n samples (a smooth map of
+    Gaussian inputs): the tensor-core training kernel alone, for measurement."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, N_IN)).astype(np.float32)
+    A = rng.standard_normal((N_IN, N_OUT)) * 0.5
+    T = (np.tanh(X @ A) + 0.1 * X[:, :N_OUT] ** 2).astype(np.float32)
+    with Closure(capacity=n) as cl:
+        cl.add_data(X, T)
+        cl.fit_normalization()
+        cl.init(seed=seed)
+        cl.train(1, batch=batch, seed=seed)          # warm-up epoch
+        t0 = time.time()
+        losses = cl.train(epochs, batch=batch, seed=seed + 1)
+        dt = time.time() - t0
+    steps = epochs * (n // batch)
+    return {"samples": n, "epochs": epochs, "batch": batch, "steps": steps, "ms_per_step": dt / steps * 1e3,
+            "samples_per_s": steps * batch / dt, "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description="learned subgrid closure: DNS -> dataset -> training -> coarse runs")
+    ap.add_argument("--synthetic-train", type=int, default=0, metavar="N",
+                    help="only time training on N synthetic samples (the tensor-core kernel alone)")
     ap.add_argument("--spinup", type=int, default=60000)
     ap.add_argument("--snapshots", type=int, default=100)
     ap.add_argument("--snap-every", type=int, default=200)
@@ -380,6 +402,9 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="write the JSON report here")
     ap.add_argument("--weights", default=None, help="save the trained closure (npz) here")
     a = ap.parse_args(argv)
+    if a.synthetic_train:
+        print(json.dumps(synthetic_train(a.synthetic_train, a.epochs, a.batch)), flush=True)
+        return 0
     res, params, norm = experiment(tuple(a.dns_grid), tuple(a.coarse_grid), a.spinup, a.snapshots, a.snap_every,
                                    a.epochs, a.batch, a.lr, log=lambda s: print(s, flush=True))
     if a.weights:
