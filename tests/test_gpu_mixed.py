@@ -107,3 +107,27 @@ def test_mixed_check_long_run_profiles_small_grid():
     assert pr["rms_rel_err"]["u"] <= 1e-3
     assert pr["uw_rel_err"] <= 1e-3
     assert r["wall_s"]["fp64"] > 0 and r["wall_s"]["mixed"] > 0
+
+
+def test_mixed_production_grid_against_fp64():
+    """Mixed precision on the benchmark grid (256, 192, 193): 50 steps against
+    the plain FP64 path from the same start, relative L2 per variable within
+    the small-grid bounds; the time-averaged wall shear within 1e-5."""
+    from compchan3dmpi_b200 import production_params, mesh_tanh, laminar_noise, cfl_dt
+    nP = (256, 192, 193)
+    x3, jac, inv = mesh_tanh(nP[2], 2.2)
+    p = production_params(nP)
+    var = laminar_noise(p, x3, seed=1234)
+    p = p.with_(dt=cfl_dt(var, p, jac, 0.6))
+    a = Channel(p.with_(mixed=True), x3, jac, inv)
+    b = Channel(p, x3, jac, inv)
+    for ch in (a, b):
+        ch.init_sol_v(var)
+        ch.time_avg_start()
+        ch.step(50)
+    e = rel_l2(a.download(), b.download())
+    assert np.all(e <= MIXED_TOL), e
+    ta, tb = a.time_average()["tau"], b.time_average()["tau"]
+    assert np.all(np.abs(ta - tb) <= 1e-5 * np.max(np.abs(tb)))
+    a.close()
+    b.close()

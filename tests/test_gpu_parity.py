@@ -93,6 +93,21 @@ def test_reference_config0_100_steps():
         _assert_close(g.download(), o.download(), what=f"config0 step {25 * (blk + 1)}")
 
 
+def test_config0_tanh_rk3_cfl05_100_steps():
+    """The 64 x 65 x 48 case as specified for the CPU-runnable comparison: tanh
+    wall stretching beta = 2, SSP-RK3 at CFL 0.5, Pr 0.72, seeded +-10% start,
+    100 steps, compared with the oracle every 25 steps."""
+    case = make_case(nP=(64, 48, 65), mesh="tanh", beta=2.0, rk=RK3, Pr=0.72, istat=10, cfl=0.5, quantize=False)
+    g, o = _pair(case)
+    for blk in range(4):
+        g.step(25)
+        o.step(25)
+        _assert_close(g.download(), o.download(), what=f"config0 tanh RK3 step {25 * (blk + 1)}")
+    gt, g1, _, _ = g.stats()
+    ot, o1, _, _ = o.stats()
+    assert np.all(np.abs(gt - ot) <= 1e-12 * np.max(np.abs(ot)))
+
+
 def test_tau_and_avg_explicit_calls():
     case = make_case(**CASES["rk3_tanh"])
     g, o = _pair(case)
@@ -310,3 +325,29 @@ def test_no_write_outside_buffers(name):
     g.fluctuation_q(np.ones((7, p.nP[2])))
     g.download()
     assert g.debug_canaries() == 0
+
+
+def test_production_grid_matches_oracle():
+    """The benchmark workload itself: nP = (256, 192, 193), tanh beta 2.2,
+    SSP-RK3 at CFL 0.6, statistics every step; two steps on the GPU against
+    the oracle on the full grid (about a second of host work)."""
+    from compchan3dmpi_b200 import production_params, mesh_tanh, laminar_noise, cfl_dt
+    nP = (256, 192, 193)
+    x3, jac, inv = mesh_tanh(nP[2], 2.2)
+    p = production_params(nP, istat=1)
+    var = laminar_noise(p, x3, seed=1234)
+    p = p.with_(dt=cfl_dt(var, p, jac, 0.6))
+    g, o = _pair((p, x3, jac, inv, var))
+    for s in (1, 2):
+        g.step(1)
+        o.step(1)
+        gv, ov = g.download(), o.download()
+        _assert_close(gv, ov, what=f"production grid step {s}")
+        del gv, ov
+    gt, g1, _, _ = g.stats()
+    ot, o1, _, _ = o.stats()
+    assert np.all(np.abs(gt - ot) <= 1e-12 * np.max(np.abs(ot)))
+    for r in range(7):
+        assert np.max(np.abs(g1[r] - o1[r])) <= 1e-12 * max(np.max(np.abs(o1[r])), 1e-300)
+    g.close()
+    o.close()
