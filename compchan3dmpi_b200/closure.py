@@ -309,7 +309,7 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     pc = pc.with_(dt=cfl_dt(varc, pc, jacc, cfl))
     window = snapshots * snap_every * pd.dt
     # DNS window: snapshots into the dataset, statistics time-averaged
-    cap = snapshots * ((dns_grid[0] - 3) // 4 + 1) * ((dns_grid[1] - 3) // 3 + 1) * ((dns_grid[2] - 1) // 3 - 1)
+    cap = snapshots * ((dns_grid[0] - 3) // 4 + 1) * ((dns_grid[1] - 3) // 3 + 1) * ((dns_grid[2] - 1) // kst - 1)
     cl = Closure(capacity=cap)
     dns.time_avg_start()
     t0 = time.time()
