@@ -393,6 +393,8 @@ int chan_closure_grad(chan_closure *m, const float *X, const float *T, int64_t n
 /* outputs in physical units for host inputs */
 int chan_closure_infer(chan_closure *m, const float *X, int64_t n, float *Y);
 const char *chan_closure_last_error(chan_closure *m);
+/* Frees the closure; contexts running with it must switch it off first
+ * (chan_set_closure(c, NULL, 0)).  NULL is allowed. */
 void chan_closure_free(chan_closure *m);
 
 /* Run a context with the closure (on = 1 or 2) or without it (on = 0).

@@ -193,3 +193,25 @@ def test_sweep_ensemble_runs_and_members_stay_finite():
         v = c.download()
         assert np.all(np.isfinite(v))
     e.close()
+
+
+def test_member_blowup_is_reported_for_that_member_only():
+    """A member whose dt is far beyond stability blows up (or turns
+    non-finite) inside the graph replays; its status says so, and the other
+    members still end bit for bit where they end alone."""
+    specs = _members()
+    good = [_open(s) for s in specs[:2]]
+    solo = [_open(s) for s in specs[:2]]
+    p, x3, jac, inv, var = specs[2][1]
+    bad = Channel(p.with_(dt=p.dt * 400), x3, jac, inv)
+    bad.init_sol_v(var)
+    e = Ensemble(good + [bad])
+    st = e.step(12)
+    assert st[0] == 0 and st[1] == 0 and st[2] in (_lib.CHAN_BLOWUP, _lib.CHAN_NONFINITE)
+    _, nstep, _ = bad.status_detail()
+    assert 1 <= nstep <= 12
+    for g in solo:
+        g.step(12)
+    for a, b in zip(good, solo):
+        assert np.array_equal(a.download(), b.download())
+    e.close()
