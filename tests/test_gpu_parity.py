@@ -83,17 +83,17 @@ def test_stats_and_forcing():
     _assert_close(g.download(), o.download(), what="after forcing")
 
 
-def test_reference_config0_100_steps():
+def test_reference_grid_64x48x65_100_steps():
     """Reference physics on the 64 x 48 x 65 grid (x, spanwise, wall-normal), 100 RK2 steps."""
     case = make_case(nP=(64, 48, 65), mesh="cosine", rk=RK2, Pr=0.71, istat=10, quantize=False)
     g, o = _pair(case)
     for blk in range(4):
         g.step(25)
         o.step(25)
-        _assert_close(g.download(), o.download(), what=f"config0 step {25 * (blk + 1)}")
+        _assert_close(g.download(), o.download(), what=f"64x48x65 step {25 * (blk + 1)}")
 
 
-def test_config0_tanh_rk3_cfl05_100_steps():
+def test_grid_64x48x65_tanh_rk3_cfl05_100_steps():
     """The 64 x 65 x 48 case as specified for the CPU-runnable comparison: tanh
     wall stretching beta = 2, SSP-RK3 at CFL 0.5, Pr 0.72, seeded +-10% start,
     100 steps, compared with the oracle every 25 steps."""
@@ -102,7 +102,7 @@ def test_config0_tanh_rk3_cfl05_100_steps():
     for blk in range(4):
         g.step(25)
         o.step(25)
-        _assert_close(g.download(), o.download(), what=f"config0 tanh RK3 step {25 * (blk + 1)}")
+        _assert_close(g.download(), o.download(), what=f"64x48x65 tanh RK3 step {25 * (blk + 1)}")
     gt, g1, _, _ = g.stats()
     ot, o1, _, _ = o.stats()
     assert np.all(np.abs(gt - ot) <= 1e-12 * np.max(np.abs(ot)))
