@@ -291,7 +291,7 @@ def _errors(les, dns):
 
 
 def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000, snapshots=100, snap_every=200,
-               epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, log=print):
+               epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, fp64_probe=400, log=print):
     t_all = time.time()
     kst = (dns_grid[2] - 1) // (coarse_grid[2] - 1)
     x3d, jacd, invd = mesh_tanh(dns_grid[2], beta)
@@ -319,6 +319,14 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     dns_wall = time.time() - t0
     avg_d = dns.time_average()
     dns_stats = _profiles(avg_d, x3d, pd.Re)
+    # plain FP64 DNS on the same GPU: time a few hundred steps from the window's end state
+    f64 = Channel(pd.with_(mixed=False), x3d, jacd, invd)
+    f64.init_sol_v(dns.download())
+    f64.step(20)
+    t0 = time.time()
+    f64.step(fp64_probe)
+    fp64_ms = (time.time() - t0) / fp64_probe * 1e3
+    f64.close()
     # the DNS statistics at the coarse grid's wall-normal points
     dns_c = {k: (np.asarray(v)[::kst].tolist() if isinstance(v, list) else v) for k, v in dns_stats.items()}
     dns.close()
@@ -355,12 +363,15 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
         ch.close()
         log(json.dumps({"phase": f"coarse {name}", "steps": nc, "wall_s": wall, "report": rep,
                         "errors": runs[name]["errors_vs_dns"]}))
+    fp64_window_s = fp64_ms * 1e-3 * snapshots * snap_every
     out = {"dns": {"nP": list(dns_grid), "dt": pd.dt, "window_steps": snapshots * snap_every, "window_t": window,
-                   "wall_s": dns_wall, "stats": dns_c},
+                   "wall_s": dns_wall, "stats": dns_c, "precision": "mixed FP32/FP64",
+                   "fp64_ms_per_step": fp64_ms, "fp64_window_s": fp64_window_s},
            "coarse": {"nP": list(coarse_grid), "runs": runs},
            "training": {"samples": cl.count, "epochs": epochs, "batch": batch, "lr": lr,
                         "losses": [float(x) for x in losses], "wall_s": train_s},
            "wall_time_ratio_dns_over_closure": dns_wall / runs["closure"]["wall_s"],
+           "wall_time_ratio_fp64_dns_over_closure": fp64_window_s / runs["closure"]["wall_s"],
            "total_s": time.time() - t_all}
     params, norm = cl.params, cl.norm
     cl.close()
