@@ -235,3 +235,32 @@ def test_stratified_start_is_at_uniform_pressure():
     assert np.allclose(v[6], 1.0 / (p.gama * p.Mac ** 2))
     assert np.allclose(v[0] * v[5], 1.0)
     assert np.allclose(v[4], v[5] + 0.5 * p.ggM * (v[1] ** 2 + v[2] ** 2 + v[3] ** 2))
+
+
+def test_closure_coarsening_and_smooth_start():
+    """The coarse start of the closure experiment: periodic linear
+    interpolation is exact on the coarse grid's own points when they are a
+    subset of the source's, every third wall-normal plane of a tanh grid is the
+    coarse tanh grid, walls come out at rest at their temperature, and E and p
+    follow from the primitives."""
+    from compchan3dmpi_b200.closure import coarsen, smooth_start, _interp_periodic
+    n = 2 + 48
+    src = np.sin(2 * np.pi * np.arange(-1, n - 1) / (n - 2))[None, :]
+    dst = _interp_periodic(src, n, 2 + 12, axis=-1)[0]
+    assert np.allclose(dst[1:-1], np.sin(2 * np.pi * np.arange(12) / 12), atol=1e-12)
+    assert dst[0] == dst[-2] and dst[-1] == dst[1]
+    pd = ChanParams(nP=(50, 26, 25), Tw=(0.9, 1.1))
+    pc = ChanParams(nP=(14, 8, 9), Tw=(0.9, 1.1))
+    x3d, _, _ = mesh_tanh(25, 2.2)
+    x3c, _, _ = mesh_tanh(9, 2.2)
+    assert np.allclose(x3d[::3], x3c)
+    v = smooth_start(pd, x3d)
+    assert np.all(np.isfinite(v)) and np.abs(v[1]).max() > 1.0
+    c = coarsen(v, pd, pc, 3)
+    assert c.shape == (7, 9, 8, 14)
+    assert np.all(c[1:4, 0] == 0) and np.all(c[1:4, -1] == 0)
+    assert np.all(c[5, 0] == 0.9) and np.all(c[5, -1] == 1.1)
+    assert np.allclose(c[4], c[5] + 0.5 * pc.ggM * (c[1] ** 2 + c[2] ** 2 + c[3] ** 2))
+    assert np.allclose(c[6], c[0] * c[5] / (pc.gama * pc.Mac ** 2))
+    # periodic duplicates of the coarse field
+    assert np.array_equal(c[..., 0], c[..., -2]) and np.array_equal(c[..., -1], c[..., 1])
