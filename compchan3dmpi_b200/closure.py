@@ -291,7 +291,8 @@ def _errors(les, dns):
 
 
 def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000, snapshots=100, snap_every=200,
-               epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, fp64_probe=400, log=print):
+               epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, fp64_probe=400, filter_width=4,
+               log=print):
     t_all = time.time()
     kst = (dns_grid[2] - 1) // (coarse_grid[2] - 1)
     x3d, jacd, invd = mesh_tanh(dns_grid[2], beta)
@@ -315,7 +316,7 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     t0 = time.time()
     for s in range(snapshots):
         dns.step(snap_every)
-        cl.sample(dns, strides=(4, 3, kst), width=4)
+        cl.sample(dns, strides=(4, 3, kst), width=filter_width)
     dns_wall = time.time() - t0
     avg_d = dns.time_average()
     dns_stats = _profiles(avg_d, x3d, pd.Re)
@@ -368,7 +369,7 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
                    "wall_s": dns_wall, "stats": dns_c, "precision": "mixed FP32/FP64",
                    "fp64_ms_per_step": fp64_ms, "fp64_window_s": fp64_window_s},
            "coarse": {"nP": list(coarse_grid), "runs": runs},
-           "training": {"samples": cl.count, "epochs": epochs, "batch": batch, "lr": lr,
+           "training": {"samples": cl.count, "epochs": epochs, "batch": batch, "lr": lr, "filter_width": filter_width,
                         "losses": [float(x) for x in losses], "wall_s": train_s},
            "wall_time_ratio_dns_over_closure": dns_wall / runs["closure"]["wall_s"],
            "wall_time_ratio_fp64_dns_over_closure": fp64_window_s / runs["closure"]["wall_s"],
@@ -410,6 +411,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--dns-grid", type=int, nargs=3, default=[256, 192, 193])
     ap.add_argument("--coarse-grid", type=int, nargs=3, default=[64, 64, 65])
+    ap.add_argument("--filter-width", type=int, default=4,
+                    help="box-filter width (even, in DNS points) in x and spanwise for the training targets")
     ap.add_argument("--out", default=None, help="write the JSON report here")
     ap.add_argument("--weights", default=None, help="save the trained closure (npz) here")
     a = ap.parse_args(argv)
@@ -417,7 +420,8 @@ def main(argv=None):
         print(json.dumps(synthetic_train(a.synthetic_train, a.epochs, a.batch)), flush=True)
         return 0
     res, params, norm = experiment(tuple(a.dns_grid), tuple(a.coarse_grid), a.spinup, a.snapshots, a.snap_every,
-                                   a.epochs, a.batch, a.lr, log=lambda s: print(s, flush=True))
+                                   a.epochs, a.batch, a.lr, filter_width=a.filter_width,
+                                   log=lambda s: print(s, flush=True))
     if a.weights:
         np.savez(a.weights, params=params, norm=norm)
     s = json.dumps(res)
