@@ -184,11 +184,15 @@ def run_with_fallback(ch: Channel, cl: Closure, steps: int, check_every: int = 1
     """``steps`` steps with the closure, checking every ``check_every`` steps.
     On divergence (blow-up, non-finite state, or the closure's output flag)
     the last good checkpoint is restored and the remaining steps run with the
-    plain method.  Returns {"fallback_step": step or None, "reason": ...}."""
+    plain method.  Returns {"fallback_step": step or None, "reason": ...}.
+    The checkpoint lives in ``workdir``, or in a temporary directory removed
+    on return."""
+    if workdir is None:
+        with tempfile.TemporaryDirectory(prefix="closure_") as tmp:
+            return run_with_fallback(ch, cl, steps, check_every, tmp)
     attach(ch, cl, True)
     closure_flag(ch, reset=True)
-    wd = workdir or tempfile.mkdtemp(prefix="closure_")
-    ckp = os.path.join(wd, "last_good.ckp")
+    ckp = os.path.join(workdir, "last_good.ckp")
     ch.checkpoint_write(ckp)
     done, report = 0, {"fallback_step": None, "reason": None}
     while done < steps:
