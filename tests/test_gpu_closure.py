@@ -206,3 +206,18 @@ def test_closure_once_per_step_and_every_stage():
     assert np.all(np.isfinite(va)) and np.all(np.isfinite(vb))
     assert not np.array_equal(va, vb)
     assert np.max(np.abs(va - vb)) < 5e-2 * np.max(np.abs(vb))
+
+
+def test_fallback_without_a_workdir_leaves_no_files(monkeypatch, tmp_path):
+    """With no workdir the last good checkpoint lives in a temporary directory
+    that is removed on return."""
+    import tempfile
+    monkeypatch.setattr(tempfile, "tempdir", str(tmp_path))
+    p, x3, jac, inv, var = _dns_case()
+    cl, params, norm = _random_closure(seed=33)
+    cl.params = params * 1e3
+    g = Channel(p, x3, jac, inv)
+    g.init_sol_v(var)
+    rep = run_with_fallback(g, cl, steps=8, check_every=4)
+    assert rep["reason"] is not None and g.nstep == 8
+    assert list(tmp_path.iterdir()) == []

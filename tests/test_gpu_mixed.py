@@ -131,3 +131,37 @@ def test_mixed_production_grid_against_fp64():
     assert np.all(np.abs(ta - tb) <= 1e-5 * np.max(np.abs(tb)))
     a.close()
     b.close()
+
+
+def test_mixed_with_the_reference_rk2_scheme():
+    """Mixed precision under the reference's two-stage RK (stage 1 double in,
+    float out; stage 2 float in, double out) against the oracle over 100 steps
+    of the reference grid's physics on a small grid."""
+    from compchan3dmpi_b200 import RK2
+    p, x3, jac, inv, var = make_case(nP=(32, 24, 33), mesh="cosine", rk=RK2, Pr=0.71, istat=10, cfl=0.5)
+    g = Channel(p.with_(mixed=True), x3, jac, inv)
+    g.init_sol_v(var)
+    o = O.Oracle(p, x3, jac, inv)
+    o.upload(var)
+    for blk in range(4):
+        g.step(25)
+        o.step(25)
+        e = rel_l2(g.download(), o.download())
+        assert np.all(e <= MIXED_TOL), (25 * (blk + 1), e)
+    assert e.max() > 0.0
+
+
+def test_mixed_buoyancy_tracks_fp64():
+    """The buoyancy term on the mixed path (computed in double from the float
+    stage state) against the plain FP64 path with the same term."""
+    from compchan3dmpi_b200.ensemble import stratified_start
+    p, x3, jac, inv, _ = make_case(nP=(24, 16, 21), mesh="tanh", beta=2.2, rk=RK3, Pr=0.72, istat=5, quantize=False)
+    p = p.with_(Tw=(0.9, 1.1))
+    var = stratified_start(p, x3, 0.9, 1.1, seed=99)
+    a = Channel(p.with_(mixed=True), x3, jac, inv)
+    b = Channel(p, x3, jac, inv)
+    for ch in (a, b):
+        ch.set_buoyancy(0.5, 1.0)
+        ch.init_sol_v(var)
+        ch.step(40)
+    assert np.all(rel_l2(a.download(), b.download()) <= MIXED_TOL)
