@@ -73,55 +73,110 @@ def config_dict(p, n_gpus):
 
 # --------------------------------------------------------------- clocks
 class Clocks:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled during the timed region.
 
-    def __init__(self, gpu: int):
+    NVML (the library behind nvidia-smi) is polled every few milliseconds from
+    a thread, so that even a timed region of a few tens of milliseconds gets
+    samples; nvidia-smi's own loop (200 ms at best, block-buffered when piped)
+    is the fallback.  Only reads: no clock or other setting is changed."""
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
+
+    def __init__(self, gpu: int, period_s: float = 0.004):
         self.gpu = gpu
-        self.proc = None
-        self.lines = []
+        self.period = period_s
+        self.sm, self.mx, self.bits = [], [], []
+        self.nv = self.h = None
+        self._stop = threading.Event()
+        self.t = None
+        self.source = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.gpu)
+        try:
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip().isdigit()]
+            idx = int(ids[self.gpu]) if self.gpu < len(ids) else self.gpu
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        self.sm.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+        self.mx.append(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        self.bits.append(int(nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            self._stop.wait(self.period)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
-                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.nv, self.h = self._handle()
+            self._sample()
+            self.source = "nvml"
+        except Exception:
+            self.nv = None
+            return self._start_smi()
+        self.t = threading.Thread(target=self._loop, daemon=True)
+        self.t.start()
+
+    def _start_smi(self):
+        fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True, bufsize=1)
+            self.source = "nvidia-smi"
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
 
-    def _read(self):
+    def _read_smi(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm, mx = float(f[0]), float(f[1])
+            except (ValueError, IndexError):
+                continue
+            b = 0
+            for (name, bit), v in zip(self.REASONS, f[2:6]):
+                if v.lower() == "active":
+                    b |= bit
+            self.sm.append(sm); self.mx.append(mx); self.bits.append(b)
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, mx, reasons = [], [], set()
-        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
+        self._stop.set()
+        if self.source == "nvml":
+            self.t.join(timeout=2)
             try:
-                sm.append(float(f[1])); mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names[1:], f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                self._sample()   # one more sample at the end of the region
+            except Exception:
+                pass
+        elif self.source == "nvidia-smi" and self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+        if not self.sm:
+            return None
+        reasons = sorted({name for b in self.bits for name, bit in self.REASONS if b & bit})
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": max(self.mx), "reasons": reasons,
+                "samples": len(self.sm), "source": self.source}
 
 
 # --------------------------------------------------------------- peaks
@@ -135,19 +190,19 @@ def hbm_peak():
 
 
 def measured_traffic(p, n_int):
-    """Per-launch DRAM bytes of the stage kernel: the per-point figure of the
-    committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum over
-    one RK3 step of a 4.6 M-point case) scaled by this workload's points."""
-    name = "stage_kernel_mixed_256x192x97_full.md" if getattr(p, "mixed", False) else "stage_kernel_256x192x97_full.md"
-    f = os.path.join(ROOT, "profiles", name)
+    """Per-launch DRAM bytes of the stage kernel: the per-point figure that
+    profiles/stage_kernel_traffic.json records from an ncu capture
+    (dram__bytes_read.sum + dram__bytes_write.sum over one RK3 step of a
+    smaller grid, per updated point and launch) scaled by this workload's
+    updated points.  Returns (bytes or None, provenance)."""
+    f = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    key = "mixed" if getattr(p, "mixed", False) else "fp64"
     try:
         with open(f) as fh:
-            for ln in fh:
-                if ln.startswith("traffic_bytes_per_updated_point_per_launch"):
-                    return float(ln.split("=")[1]) * n_int
-    except (OSError, ValueError):
-        return None
-    return None
+            rec = json.load(fh)[key]
+        return float(rec["bytes_per_updated_point_per_launch"]) * n_int, rec.get("capture")
+    except (OSError, KeyError, ValueError, TypeError):
+        return None, None
 
 
 # --------------------------------------------------------------- CPU
@@ -234,7 +289,8 @@ def run_reference(args):
     val = p.n_interior * K / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / K * 1e3 * p.stages,
+        "steps": K, "warmup": W, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": dt / K * 1e3 * p.stages,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded laminar Poiseuille +-10%)", "config": config_dict(p, 1),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
@@ -338,7 +394,7 @@ def run_ours(args):
             bpp = (80 + 120 * (stages - 1)) / stages   # algorithmic bytes per updated point per stage launch
         achieved = n_int * bpp / (stage_ms_max / 1e3) / 1e9
         peak, peak_kind = hbm_peak()
-        traffic = measured_traffic(p, n_int)
+        traffic, traffic_src = measured_traffic(p, n_int)
         # stage + wall-BC kernels per stage, plus the two statistics passes on their cadence
         launches = K * 2 * stages + 2 * sum(1 for s in range(W + 1, W + K + 1) if s % p.istat == 0)
         line = {
@@ -347,7 +403,7 @@ def run_ours(args):
             "dtype": "f32+f64" if p.mixed else "f64", "data": "synthetic (seeded laminar Poiseuille +-10%)",
             "config": config_dict(p, ranks.world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                          "kernel": "k_stage<32,8>", "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": n_int * bpp,
                          "stage_kernel_ms": stage_ms_max,
@@ -355,9 +411,10 @@ def run_ours(args):
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                     "calls": "chan_upload(var) + K/istat x chan_step(istat) + chan_stats every istat + chan_download(var)"},
             "gpu_launches": int(launches),
-            "clocks": ck,
             "status_ok": status_ok,
         }
+        if ck:
+            line["clocks"] = ck
         if p.mixed:
             line["mixed_error"] = mixed_error(p, x3, jac, inv, var)
         if ranks.world == 1 and not args.no_cpu_baseline:
@@ -475,9 +532,10 @@ def run_ensemble(args):
                              "member (host wall clock around the synchronous calls)"},
             "gpu_launches": int(launches),
             "graph": {"replays": replays, "captures": captures},
-            "clocks": ck,
             "status_ok": all(x == 0 for x in st0 + st1 + st2),
         }
+        if ck:
+            line["clocks"] = ck
         print(json.dumps(line), flush=True)
     R.finalize(ranks)
     return 0

@@ -184,9 +184,11 @@ def run_with_fallback(ch: Channel, cl: Closure, steps: int, check_every: int = 1
     """``steps`` steps with the closure, checking every ``check_every`` steps.
     On divergence (blow-up, non-finite state, or the closure's output flag)
     the last good checkpoint is restored and the remaining steps run with the
-    plain method.  Returns {"fallback_step": step or None, "reason": ...}.
-    The checkpoint lives in ``workdir``, or in a temporary directory removed
-    on return."""
+    plain method.  Returns {"fallback_step": step or None, "reason": ...,
+    "plain_failed": None or the plain method's own failure}: if the plain
+    continuation blows up too, the report says so (with its step) instead of
+    the exception replacing it.  The checkpoint lives in ``workdir``, or in a
+    temporary directory removed on return."""
     if workdir is None:
         with tempfile.TemporaryDirectory(prefix="closure_") as tmp:
             return run_with_fallback(ch, cl, steps, check_every, tmp)
@@ -194,7 +196,7 @@ def run_with_fallback(ch: Channel, cl: Closure, steps: int, check_every: int = 1
     closure_flag(ch, reset=True)
     ckp = os.path.join(workdir, "last_good.ckp")
     ch.checkpoint_write(ckp)
-    done, report = 0, {"fallback_step": None, "reason": None}
+    done, report = 0, {"fallback_step": None, "reason": None, "plain_failed": None}
     while done < steps:
         n = min(check_every, steps - done)
         reason = None
@@ -209,8 +211,12 @@ def run_with_fallback(ch: Channel, cl: Closure, steps: int, check_every: int = 1
         if reason is not None:
             ch.checkpoint_read(ckp)
             attach(ch, None, False)
-            report = {"fallback_step": int(ch.nstep), "reason": reason}
-            ch.step(steps - done)
+            report = {"fallback_step": int(ch.nstep), "reason": reason, "plain_failed": None}
+            try:
+                if ch.step(steps - done):
+                    report["plain_failed"] = {"reason": "non-finite state", "step": int(ch.nstep)}
+            except BlowUpError as e:
+                report["plain_failed"] = {"reason": "blow-up", "step": int(e.nstep), "ijk": list(e.ijk)}
             return report
         done += n
         ch.checkpoint_write(ckp)

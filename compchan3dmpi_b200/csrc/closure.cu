@@ -51,7 +51,11 @@ __global__ void __launch_bounds__(128, 1)
     }
     const bool ok = umma::mbar_wait(&mbar, 0, kWaitLimit);
     if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
+        // give the MMA one more bounded wait before its tensor memory is freed
+        if (tid == 0) {
+            atomicExch(err, 1);
+            umma::mbar_wait(&mbar, 0, kWaitLimit);
+        }
     } else {
         umma::fence_after_sync();
         for (int c = 0; c < N; c += 16) {

@@ -7,7 +7,7 @@
  * (module bodies in v1.10/codes/module_comp.f90).  The monolithic form is
  * v1.9/codes/main_v1.9.f90:304-1049.
  * All entry points use plain pointers, sizes and C scalars, so a Fortran host
- * can bind them with iso_c_binding.  INTEGRATION.md gives the interface module.
+ * can bind them with iso_c_binding through a bind(c) interface module.
  *
  * Axes and arrays follow the reference exactly.
  *   index 1 (i, nP[0]) : streamwise x, periodic.
@@ -247,7 +247,10 @@ int chan_set_buoyancy(chan_ctx *c, double Ri, double Tref);
  * time-averaging sums.  Restarting from it continues bit for bit.  The
  * reference restarts from its Tecplot deck with the forcing reset to zero
  * (v1.9/codes/main_v1.9.f90:211-282, 749-794); this sidecar has no
- * counterpart there.  chan_checkpoint_read needs a context of the same grid. */
+ * counterpart there.  chan_checkpoint_read needs a context of the same grid,
+ * x3 mesh, physics (Re, Mac, Pr, gama, Pe, Lx, Ly, Tw), dt, RK scheme, forcing
+ * and precision; it returns CHAN_EINVAL, naming the first field that
+ * differs in chan_last_error, and leaves the context as it was otherwise. */
 int chan_checkpoint_write(chan_ctx *c, const char *path);
 int chan_checkpoint_read(chan_ctx *c, const char *path);
 
@@ -276,7 +279,7 @@ const char *chan_io_last_error(void);
  * static device array of CHAN_NOALLOC_MAX_DOUBLES doubles (32 MiB), which
  * every GPU that loads the library holds until the process exits.
  * The results equal chan_avg_spatial + chan_stats on the same field
- * (v1.9/codes/main_v1.9.f90:995-1025 semantics: sums over i=1..nP1,
+ * (v1.9/codes/main_v1.9.f90:972-1002 semantics: sums over i=1..nP1,
  * j=1..nP2 divided by nP1*nP2).
  *
  * var    : var(1:nP1,1:nP2,1:nP3,1:7) in host memory.
@@ -285,8 +288,9 @@ const char *chan_io_last_error(void);
  * Limit  : 23*nP3 (rounded up to 32) + 7*nP1*nP2 <= CHAN_NOALLOC_MAX_DOUBLES,
  *          i.e. one full wall-normal plane of all seven variables must fit;
  *          larger grids return CHAN_EINVAL with a message (chan_last_error(NULL)).
- * The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress, no allocation); make that first call before any
+ * Every call looks up the array's device address in the device's current
+ * context (cudaGetSymbolAddress, no allocation); the first call on a device
+ * may also load the library's device code there, so make it before any
  * stream capture.  It works on the legacy default stream and synchronizes
  * it.  It restores the calling thread's current device on return.
  * All calls share the one array: calls that overlap on the GPU (concurrent

@@ -6,14 +6,16 @@ next to the exact derivative
 (v1.8_validation/codes/mainV1.8_serial.f90:76-105, 808-824).  The captured
 output is v1.8_validation/codes/nohupDebug.out:23-26.
 
-Run in a container that has the reference mounted:
-    python tests/golden/make_kat_fixture.py /root/reference
+Run where the reference is checked out, giving its root directory:
+    python tests/golden/make_kat_fixture.py <reference-root>
 """
 import json
 import sys
 from pathlib import Path
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_kat_fixture.py <reference-root>")
+ref = Path(sys.argv[1])
 lines = (ref / "v1.8_validation/codes/nohupDebug.out").read_text().splitlines()
 rows = {}
 for ln in lines[22:26]:

@@ -177,6 +177,7 @@ def test_divergent_closure_falls_back_to_the_plain_method(tmp_path):
     g.init_sol_v(var)
     rep = run_with_fallback(g, cl, steps=12, check_every=4, workdir=str(tmp_path))
     assert rep["fallback_step"] is not None and rep["reason"] is not None
+    assert rep["plain_failed"] is None
     assert g.nstep == 12 and g.status() == 0
     assert np.all(np.isfinite(g.download()))
     # the plain method from the same start gives the same state

@@ -274,6 +274,14 @@ def test_checkpoint_faults_are_codes(tmp_path):
     with pytest.raises(ChanError) as ei:
         b.checkpoint_read(good)
     assert ei.value.code == -1
+    # same grid, other physics or method: refused, naming the field
+    for change, field in ((dict(dt=p.dt * 0.5), "dt"), (dict(Re=p.Re + 1.0), "Re"),
+                          (dict(rk_scheme=3 if p.rk_scheme == 2 else 2), "rk_scheme")):
+        d = Channel(p.with_(**change), x3, jac, inv)
+        with pytest.raises(ChanError) as ei:
+            d.checkpoint_read(good)
+        assert ei.value.code == -1 and field in str(ei.value), (change, str(ei.value))
+        d.close()
     a.step(1)   # still usable
     assert a.nstep == 3
 
