@@ -11,7 +11,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -490,24 +489,19 @@ int dalloc(chan_ctx *c, double **p, size_t n)
 // overlap on the GPU (two host threads, or two streams) race on it.
 static __device__ __align__(256) double g_noalloc_scratch[CHAN_NOALLOC_MAX_DOUBLES];
 
-std::mutex g_noalloc_mu;
-double *g_noalloc_addr[256] = {nullptr};  // device address of the array, per device
-
-// device address of g_noalloc_scratch on the current device; resolved once per device
-double *noalloc_scratch(int dev)
+// device address of g_noalloc_scratch in the current device's context.  It is
+// looked up on every call (cudaGetSymbolAddress allocates nothing): an address
+// kept from an earlier call would go stale if the context were reset and
+// re-created in between.
+double *noalloc_scratch()
 {
-    if (dev < 0 || dev >= 256) return nullptr;
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            g_init_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-            return nullptr;
-        }
-        g_noalloc_addr[dev] = (double *)p;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        g_init_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return nullptr;
     }
-    return g_noalloc_addr[dev];
+    return (double *)p;
 }
 
 // blocks per plane of the statistics pass: about 16 blocks per SM, at least
@@ -931,7 +925,7 @@ int64_t chan_device_bytes(chan_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
 // ghosts, the wall planes, the stale corner columns, the forcing/statistics
 // state and the counters, in native byte order.
 namespace {
-const char kCkpMagic[8] = {'C', 'H', 'A', 'N', 'C', 'K', 'P', '1'};
+const char kCkpMagic[8] = {'C', 'H', 'A', 'N', 'C', 'K', 'P', '2'};
 struct CkpHeader {
     char magic[8];
     int32_t nP[3];
@@ -942,7 +936,52 @@ struct CkpHeader {
     double tavg_t0, tavg_t1;
     int32_t acc_on;
     int32_t pad;
+    // the run's physics and method: a restart into a context that differs in
+    // any of them is refused instead of continuing with other physics
+    double Re, Mac, dt, Pr, gama, Pe[3], Lx, Ly, Tw[2];
+    int32_t rk_scheme, forcing, flags, pad2;
+    uint64_t x3_hash;   // FNV-1a of the x3 mesh bytes given to chan_init
 };
+
+uint64_t fnv1a(const void *data, size_t n)
+{
+    const unsigned char *b = static_cast<const unsigned char *>(data);
+    uint64_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+void ckp_fill_physics(const chan_ctx *c, CkpHeader &h)
+{
+    const chan_params &p = c->p;
+    h.Re = p.Re; h.Mac = p.Mac; h.dt = p.dt; h.Pr = p.Pr; h.gama = p.gama;
+    for (int m = 0; m < 3; m++) h.Pe[m] = p.Pe[m];
+    h.Lx = p.Lx; h.Ly = p.Ly; h.Tw[0] = p.Tw[0]; h.Tw[1] = p.Tw[1];
+    h.rk_scheme = p.rk_scheme; h.forcing = p.forcing; h.flags = p.flags;
+    h.x3_hash = fnv1a(c->hx3.data(), c->hx3.size() * sizeof(double));
+}
+
+// name of the first physics field in which two headers differ, or nullptr
+const char *ckp_physics_mismatch(const CkpHeader &a, const CkpHeader &b)
+{
+    if (a.Re != b.Re) return "Re";
+    if (a.Mac != b.Mac) return "Mac";
+    if (a.dt != b.dt) return "dt";
+    if (a.Pr != b.Pr) return "Pr";
+    if (a.gama != b.gama) return "gama";
+    for (int m = 0; m < 3; m++)
+        if (a.Pe[m] != b.Pe[m]) return "Pe";
+    if (a.Lx != b.Lx || a.Ly != b.Ly) return "Lx/Ly";
+    if (a.Tw[0] != b.Tw[0] || a.Tw[1] != b.Tw[1]) return "Tw";
+    if (a.rk_scheme != b.rk_scheme) return "rk_scheme";
+    if (a.forcing != b.forcing) return "forcing";
+    if (a.flags != b.flags) return "flags (precision)";
+    if (a.x3_hash != b.x3_hash) return "x3 mesh";
+    return nullptr;
+}
 }  // namespace
 
 int chan_checkpoint_write(chan_ctx *c, const char *path)
@@ -958,6 +997,7 @@ int chan_checkpoint_write(chan_ctx *c, const char *path)
     for (int m = 0; m < 3; m++) h.nP[m] = c->p.nP[m];
     h.px = c->px; h.nstep = c->nstep; h.time = c->time;
     h.tavg_samples = c->tavg_samples; h.tavg_t0 = c->tavg_t0; h.tavg_t1 = c->tavg_t1; h.acc_on = c->kp.acc_on;
+    ckp_fill_physics(c, h);
     const size_t nq = 5 * (size_t)c->vol, nw = 16 * (size_t)c->plane, ncs = (size_t)(c->n3 + 2) * 28,
                  nst = 23 * (size_t)c->n3 + 2;
     std::vector<double> hb(nq + nw + ncs + 2 * nst);
@@ -992,6 +1032,15 @@ int chan_checkpoint_read(chan_ctx *c, const char *path)
         fclose(f);
         c->err = "checkpoint grid differs from the context's";
         return CHAN_EINVAL;
+    }
+    {
+        CkpHeader mine{};
+        ckp_fill_physics(c, mine);
+        if (const char *what = ckp_physics_mismatch(h, mine)) {
+            fclose(f);
+            c->err = std::string("checkpoint physics differ from the context's: ") + what;
+            return CHAN_EINVAL;
+        }
     }
     const size_t nq = 5 * (size_t)c->vol, nw = 16 * (size_t)c->plane, ncs = (size_t)(c->n3 + 2) * 28,
                  nst = 23 * (size_t)c->n3 + 2;
@@ -1187,7 +1236,7 @@ int chan_avg_spatial_noalloc(const double *var, const int32_t *nP, double *stat1
     if (cudaGetDevice(&prev) != cudaSuccess) prev = device;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) { g_init_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return CHAN_ECUDA; }
-    double *scr = noalloc_scratch(device);
+    double *scr = noalloc_scratch();
     if (!scr) { cudaSetDevice(prev); return CHAN_ECUDA; }
     double *res = scr, *slab = scr + head;
     int sms = 148;
