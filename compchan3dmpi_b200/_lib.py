@@ -111,6 +111,9 @@ SIGNATURES = [
     ("chan_ensemble_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _I32]),
     ("chan_ensemble_tune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _D]),
     ("chan_ensemble_counters", ctypes.c_int, [ctypes.c_void_p, _I64, _I64, _D]),
+    ("chan_ensemble_set_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("chan_ensemble_get_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.POINTER(ctypes.c_char_p)]),
     ("chan_ensemble_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("chan_ensemble_free", None, [ctypes.c_void_p]),
     ("chan_selftest_umma", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16),
@@ -143,6 +146,9 @@ CHAN_TILE_32x8 = 0
 CHAN_TILE_32x4 = 1
 CHAN_TILE_16x16 = 2
 CHAN_NTILES = 3
+CHAN_ENSEMBLE_GRAPH = 0
+CHAN_ENSEMBLE_PERSISTENT = 1
+CHAN_ENSEMBLE_PERSISTENT_STALL_TEST = 2
 
 _lib = None
 

@@ -18,6 +18,7 @@
 // pressure BC).  k_stats_part + k_stats_fin run every istat steps.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <type_traits>
@@ -38,7 +39,8 @@ struct DevStatus {
     int nonfinite;         // NaN/Inf seen
     int nf_ijk[3];
     long long blown_step;  // step in which the blow-up happened
-    long long pad;
+    int stall;             // 1: a stage kernel's bulk copy did not complete in time; 2: misaligned staging area
+    int pad;
 };
 
 // Boundary condition of one wall plane (plug-in of the reference's wall-BC
@@ -254,9 +256,12 @@ __device__ __forceinline__ void gd_point(const FluxC<R> &C, R mu, R pr, R u0, R 
     g[3] = fmaR(C.ggM, fmaR(w0, g4, fmaR(v0, g3, -(u0 * t12))), -(kqm * Ty));
 }
 
+// The flux helpers below take plane t's primitives from the ring slot s, plane
+// t+1's from sp, and plane t-1's values at point b as scalars (um, vm, wm),
+// which the caller keeps outside the ring.
 template <int BX, typename R>
-__device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
-                                        const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4])
+__device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, R um, R wm, const SlotT<R> &sp,
+                                        const R *MU, const R *PR, int b, R czt, R f[4])
 {
     const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
     const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
@@ -264,14 +269,14 @@ __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, co
     const R vy = (s.V[b + BX] - s.V[b - BX]) * C.hdy;
     const R wx = (s.W[b + 1] - s.W[b - 1]) * C.hdx;
     const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
-    const R uz = (sp.U[b] - sm.U[b]) * czt;
-    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R uz = (sp.U[b] - um) * czt;
+    const R wz = (sp.W[b] - wm) * czt;
     fd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wx, uz, Tx, f);
 }
 
 template <int BX, typename R>
-__device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
-                                        const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R g[4])
+__device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, R vm, R wm, const SlotT<R> &sp,
+                                        const R *MU, const R *PR, int b, R czt, R g[4])
 {
     const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
     const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
@@ -279,16 +284,16 @@ __device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, co
     const R vy = (s.V[b + BX] - s.V[b - BX]) * C.hdy;
     const R wy = (s.W[b + BX] - s.W[b - BX]) * C.hdy;
     const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
-    const R vz = (sp.V[b] - sm.V[b]) * czt;
-    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R vz = (sp.V[b] - vm) * czt;
+    const R wz = (sp.W[b] - wm) * czt;
     gd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wy, vz, Ty, g);
 }
 
 // fD and gD together at one point: they share eight gradients, the shear
 // stress mu*(dv/dx+du/dy) (fD3 = gD2) and p + 2/3*mu*div.
 template <int BX, typename R>
-__device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, const SlotT<R> &sm,
-                                         const SlotT<R> &sp, const R *MU, const R *PR, int b, R czt, R f[4], R g[4])
+__device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, R um, R vm, R wm, const SlotT<R> &sp,
+                                         const R *MU, const R *PR, int b, R czt, R f[4], R g[4])
 {
     const R ux = (s.U[b + 1] - s.U[b - 1]) * C.hdx;
     const R uy = (s.U[b + BX] - s.U[b - BX]) * C.hdy;
@@ -298,9 +303,9 @@ __device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, c
     const R wy = (s.W[b + BX] - s.W[b - BX]) * C.hdy;
     const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
     const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
-    const R uz = (sp.U[b] - sm.U[b]) * czt;
-    const R vz = (sp.V[b] - sm.V[b]) * czt;
-    const R wz = (sp.W[b] - sm.W[b]) * czt;
+    const R uz = (sp.U[b] - um) * czt;
+    const R vz = (sp.V[b] - vm) * czt;
+    const R wz = (sp.W[b] - wm) * czt;
     const R mu = MU[b], pr = pres_at(C, s, PR, b);
     const R u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
     fd_point(C, mu, pr, u0, v0, w0, ux, vy, wz, vx, uy, wx, uz, Tx, f);
@@ -395,13 +400,22 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
 // A CTA owns a TI x TJ tile of interior (i,j) columns and marches a chunk of
 // interior planes k = kb..ke.  Shared memory holds, for the tile plus a
 // 2-point halo box ((TI+4) x (TJ+4)):
-//   prims u,v,w,T   of planes t-1, t, t+1   (3-slot ring)
-//   mu, p           of planes t, t+1        (2-slot ring)
-//   Q (5 vars)      of planes t, t+1        (2-slot ring)
+//   Q (5 vars)      of planes t, t+1, t+2   (3-slot ring; t+2 in flight)
+//   prims u,v,w,T   of planes t, t+1        (2-slot ring)
+//   mu, p           of planes t, t+1        (2-slot ring; mu only with float rings)
 //   fD, gD          of plane t on the tile plus a 1-point halo
-// Each thread keeps its own column's Q and w at t-2, t-1, t+2 and hD at
-// t-1, t, t+1 in registers.  Per output plane the CTA loads one new plane,
-// so Q is read from DRAM once per stage (halo re-reads come from L2).
+// Plane t-1 is kept where it is still read: each thread's own column (Q, u,
+// v, w) in registers, and the halo points of the halo-flux lanes in a small
+// shared array.  Each thread also keeps its own column's Q and w at t-2 and
+// hD at t-1, t, t+1 in registers.
+//
+// The Q box of each plane arrives by one tiled bulk tensor copy (TMA) issued
+// two planes ahead by one thread and completed on an mbarrier, so Q is read
+// from DRAM once per stage with no per-thread load instructions; the halo
+// re-reads of neighbouring CTAs come from L2.  Each staged box point is then
+// converted to primitives once per CTA.  The stage whose input is stored in a
+// wider type than the ring (the first stage of the mixed-precision path, double
+// in, float rings) loads its boxes with per-thread loads instead.
 //
 // Types: QI / QO are the storage types of the stage's input and output state,
 // R the type of the shared rings and of the flux arithmetic.  The plain FP64
@@ -423,12 +437,25 @@ struct StageShape {
     // float rings keep mu only and form p from rho and T where it is used;
     // FP64 rings keep (mu, p)
     static constexpr bool p_ring = sizeof(R) == 8;
-    static constexpr int words = 12 * NB + (p_ring ? 4 : 2) * NB + 10 * NB + 4 * NFX + 4 * NGY;
+    static constexpr int MPW = p_ring ? 2 : 1;                       // words per box point in the (mu, p) ring
+    // one Q slot: the 5-variable box of one plane, rounded up to 128 bytes
+    // (the alignment of a bulk tensor copy's shared-memory destination)
+    static constexpr size_t box_bytes = (size_t)5 * NB * sizeof(R);
+    static constexpr size_t qslot_bytes = (box_bytes + 127) / 128 * 128;
+    static constexpr int QSLOT = (int)(qslot_bytes / sizeof(R));     // slot stride in R elements
+    static constexpr size_t q_bytes = 3 * qslot_bytes;
+    static constexpr int pr_words = 2 * 4 * NB;
+    static constexpr int mp_words = 2 * MPW * NB;
+    static constexpr int fg_words = 4 * NFX + 4 * NGY;
     // float rings leave room to stage the RK base of every thread's own point
     // (double) by cp.async; the FP64 rings do not fit it beside two CTAs per SM
     static constexpr bool prefetch_base = sizeof(R) == 4;
-    static constexpr size_t bytes =
-        sizeof(R) * (size_t)words + (prefetch_base ? sizeof(double) * 5 * (size_t)NT : 0);
+    static constexpr size_t base_off = (q_bytes + sizeof(R) * (size_t)(pr_words + mp_words + fg_words) + 15) / 16 * 16;
+    // plane t-1 values (u or v, and w) of the halo-flux lanes' points, by lane
+    static constexpr int NHL = 32 + 2 * TI;
+    static constexpr size_t hl_off = base_off + (prefetch_base ? sizeof(double) * 5 * (size_t)NT : 0);
+    static constexpr size_t bar_off = (hl_off + sizeof(R) * 2 * (size_t)NHL + 7) / 8 * 8;
+    static constexpr size_t bytes = bar_off + 3 * sizeof(unsigned long long) + 2 * sizeof(int);
     // resident CTAs per SM the register budget is sized for: 128 (FP64) or 80
     // (float) registers per thread at 256 threads, but never more CTAs than
     // the 228 KB of shared memory per SM holds (1 KB of it reserved per CTA)
@@ -436,8 +463,6 @@ struct StageShape {
     static constexpr int minb_smem = (int)(233472 / (bytes + 1024));
     static constexpr int minb = minb_regs < minb_smem ? minb_regs : minb_smem;
 };
-
-
 
 template <typename R>
 __device__ __forceinline__ const FluxC<R> &fluxc(const KParams &P);
@@ -468,8 +493,10 @@ __device__ __forceinline__ double mu_of<double>(double T) { return pow07(T); }
 template <>
 __device__ __forceinline__ float mu_of<float>(double T) { return exp2f(0.7f * log2f((float)T)); }
 
-template <typename T>
-__device__ __forceinline__ double ldq(const T *p) { return (double)__ldg(p); }
+// a load of state written earlier in the same launch by other CTAs (the
+// persistent ensemble kernel) must not use the read-only path
+template <bool COHERENT, typename T>
+__device__ __forceinline__ double ldq_c(const T *p) { return COHERENT ? (double)*p : (double)__ldg(p); }
 
 // 8-byte asynchronous global->shared copy (no register staging)
 __device__ __forceinline__ void cp_async8(double *dst, const double *src)
@@ -481,34 +508,118 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int TI, int TJ, typename QI, typename QO, typename R, bool BUOY>
-__global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(const KParams P)
+// ---- tiled bulk tensor copies into this CTA's shared memory, with mbarriers
+__device__ __forceinline__ unsigned smem_u32addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init_one(unsigned long long *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32addr(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// order the CTA's earlier generic-proxy accesses of shared memory (made
+// visible to this thread by a CTA barrier) before its later async-proxy writes
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// the 4-D box at (x, y, z, w) of the tensor map into dst; bytes = box size.
+// No multicast: the box lands in this CTA's shared memory only.
+__device__ __forceinline__ void tma_load_box(void *dst, const CUtensorMap *map, int x, int y, int z, int w,
+                                             unsigned long long *bar, unsigned bytes)
+{
+    const unsigned b = smem_u32addr(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32addr(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(b)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(unsigned a, unsigned parity)
+{
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for phase `parity` of the barrier; false when about a second passed
+// without it (the caller records the error and stops)
+constexpr unsigned long long kCopyWaitNs = 1000000000ull;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity)
+{
+    const unsigned a = smem_u32addr(bar);
+    if (mbar_try(a, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(a, parity))
+        if (global_ns() - t0 > kCopyWaitNs) return false;
+    return true;
+}
+
+// One CTA's work of the stage kernel on tile (bx, by) and k-chunk bz, for
+// thread (tx, ty).  BUOYM: 0 no buoyancy term, 1 with it, 2 as P.buoy_on
+// says.  PERSIST: called from the persistent ensemble kernel, where the state
+// was written earlier in the same launch: coherent loads instead of the
+// read-only path, and a proxy fence before the first box copy.
+template <int TI, int TJ, typename QI, typename QO, typename R, int BUOYM, bool PERSIST>
+__device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *tmq, int bx, int by, int bz, int tx,
+                                           int ty, unsigned char *smem_raw)
 {
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
-    constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT;
+    constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT, MPW = S::MPW, QSLOT = S::QSLOT;
+    // boxes by bulk tensor copy when the input is stored in the ring type
+    constexpr bool TMA = std::is_same<QI, R>::value;
     static_assert(2 * TJ <= 32 && 32 + 2 * TI <= NT, "halo-flux lane layout needs 2*TJ <= 32 and 32+2*TI <= TI*TJ");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *sPr = reinterpret_cast<R *>(smem_raw);   // [3][4][NB]
-    R *sMP = sPr + 12 * NB;                     // [2][2][NB] mu, p  ([2][NB] mu with float rings)
-    R *sQ = sMP + (S::p_ring ? 4 : 2) * NB;     // [2][5][NB]
-    R *sF = sQ + 10 * NB;                       // [4][TJ][TI+2]
-    R *sG = sF + 4 * S::NFX;                    // [4][TJ+2][TI]
-    double *sQB = reinterpret_cast<double *>(smem_raw + sizeof(R) * S::words);   // [5][NT] (float rings only)
-    __shared__ int s_frozen;
+    R *sQ = reinterpret_cast<R *>(smem_raw);                       // [3 slots][5][NB]
+    R *sPr = reinterpret_cast<R *>(smem_raw + S::q_bytes);         // [2][4][NB] u,v,w,T
+    R *sMP = sPr + S::pr_words;                                    // [2][MPW][NB] mu (, p)
+    R *sF = sMP + S::mp_words;                                     // [4][TJ][TI+2]
+    R *sG = sF + 4 * S::NFX;                                       // [4][TJ+2][TI]
+    double *sQB = reinterpret_cast<double *>(smem_raw + S::base_off);   // [5][NT] (float rings only)
+    R *sH = reinterpret_cast<R *>(smem_raw + S::hl_off);                // [2][NHL]
+    // (the 8-byte rounding is a no-op: bar_off is a multiple of 8)
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(reinterpret_cast<size_t>(smem_raw + S::bar_off) & ~(size_t)7);   // [3]
+    int *sflag = reinterpret_cast<int *>(bar + 3);   // [0] the CTA leaves at once, [1] Q slots with a copy in flight
     const FluxC<R> &C = fluxc<R>(P);
     // the state pointers are read from the parameter space at each use: held
     // in registers across the kernel they cost spills
     auto qin = [&]() { return static_cast<const QI *>(P.qin); };
     auto qout = [&]() { return static_cast<QO *>(P.qout); };
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
-    if (tid == 0) s_frozen = frozen(P.status, kstep(P)) ? 1 : 0;
+    const bool buoy = BUOYM == 2 ? P.buoy_on != 0 : BUOYM == 1;
+    const int tid = ty * TI + tx;
+    if (tid == 0) {
+        sflag[0] = frozen(P.status, kstep(P)) ? 1 : 0;
+        sflag[1] = 0;
+        // state written by other CTAs of this launch, read next by box copies
+        if (PERSIST) asm volatile("fence.proxy.async.global;" ::: "memory");
+        // a bulk copy needs a 128-byte aligned destination
+        if (TMA && (smem_u32addr(smem_raw) & 127u)) {
+            sflag[0] = 1;
+            atomicExch(&P.status->stall, 2);
+        }
+        if (TMA) {
+            for (int s = 0; s < 3; s++) mbar_init_one(&bar[s]);
+            fence_mbar_init();
+        }
+    }
     __syncthreads();
-    if (s_frozen) return;
+    if (sflag[0]) return;
 
-    const int i0 = 2 + blockIdx.x * TI, j0 = 2 + blockIdx.y * TJ;
-    const int kb = 2 + blockIdx.z * P.kchunk;
+    const int i0 = 2 + bx * TI, j0 = 2 + by * TJ;
+    const int kb = 2 + bz * P.kchunk;
     const int ke = min(kb + P.kchunk - 1, P.n3 - 1);
     if (kb > ke) return;
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
@@ -519,22 +630,49 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
     const long long vol = P.vol, plane = P.plane;
     const long long colo = (long long)j * P.px + i;
 
-    // ring slots by role, rotated once per plane instead of indexed by plane:
-    // prims (u,v,w,T) for t-1, t, t+1 at offsets oM, oZ, oP; Q and (mu,p) for
-    // t, t+1 at qZ, qP and mZ, mP (offsets in words)
-    int oM = 0, oZ = 4 * NB, oP = 8 * NB, qZ = 0, qP = 5 * NB, mZ = 0, mP = (S::p_ring ? 2 : 1) * NB;
+    // ring slots by role, rotated once per plane: Q slots (indices 0..2) of
+    // planes t, t+1, t+2; prims offsets of t, t+1; (mu,p) offsets of t, t+1
+    int iZ = 1, iP = 2, iN = 0;
+    int pZ = 0, pP = 4 * NB, mZ = 0, mP = MPW * NB;
+    unsigned ph = 0u;   // parity of the next wait, per Q slot
     auto slot = [&](int o) -> Slot {
         return Slot{sPr + o, sPr + o + NB, sPr + o + 2 * NB, sPr + o + 3 * NB};
     };
     auto smu = [&](int o) { return sMP + o; };
-    auto sq = [&](int o, int v) { return sQ + o + v * NB; };
+    auto sq = [&](int s, int v) { return sQ + s * QSLOT + v * NB; };
     // what the flux helpers read the pressure from (pres_at): the p slot of
-    // the (mu,p) ring at mo, or the density of the Q ring at qo
-    auto spr = [&](int mo, int qo) { return S::p_ring ? sMP + mo + NB : sq(qo, 0); };
+    // the (mu,p) ring at mo, or the density of the Q slot s
+    auto spr = [&](int mo, int s) { return S::p_ring ? sMP + mo + NB : sq(s, 0); };
 
-    // box points this thread loads: the same columns for every plane
+    // plane m's Q box into Q slot s (one thread; bulk tensor copy)
+    auto issue = [&](int m, int s) {
+        if (TMA && tid == 0) {
+            fence_proxy_async_smem();
+            tma_load_box(sq(s, 0), tmq, i0 - 2, j0 - 2, m, 0, &bar[s], (unsigned)S::box_bytes);
+            sflag[1] |= 1 << s;
+        }
+    };
+    // wait for Q slot s; false if the copy did not complete in time
+    auto wait_slot = [&](int s) -> bool {
+        if (!TMA) return true;
+        const bool ok = mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
+        ph ^= 1u << s;
+        if (ok && tid == 0) sflag[1] &= ~(1 << s);
+        return ok;
+    };
+    // after a timed-out copy: record it, give every copy still in flight one
+    // more bounded wait (so that none lands after the CTA has left), leave
+    auto give_up = [&]() {
+        if (tid == 0) {
+            atomicExch(&P.status->stall, 1);
+            for (int s = 0; s < 3; s++)
+                if (sflag[1] & (1 << s)) mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
+        }
+    };
+
+    // box points this thread converts: the same columns for every plane
     // lp: box index | 0x10000 if the point is in R1 (tile plus a 1-point cross
-    // halo, where mu is needed); -1 if outside the array.  lo: column offset.
+    // halo, where mu and p are needed); -1 if outside the array.  lo: column offset.
     constexpr int NL = (NB + NT - 1) / NT;
     int lp[NL];
     int lo[NL];
@@ -550,15 +688,16 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
         lo[l] = gj * P.px + gi;
     }
 
-    // fill the ring slots of plane m over the whole box.  A wall plane's box
-    // holds, at periodic duplicates and ghosts, the values of their image
-    // points: the viscous fluxes next to a wall read the wall only there, and
-    // the reference's flux at a duplicate column or row is the exchanged flux
-    // of its image (whose wall values may differ from the duplicate's own
+    // primitives (and mu, p on R1) of plane m over the box, from its Q box in
+    // slot s (with per-thread loads, Q is first loaded into the slot).  A wall
+    // plane's box holds, at periodic duplicates and ghosts, the values of their
+    // image points: the viscous fluxes next to a wall read the wall only there,
+    // and the reference's flux at a duplicate column or row is the exchanged
+    // flux of its image (whose wall values may differ from the duplicate's own
     // under a non-periodic wall BC).  hD on a wall plane reads the wall's own
     // values from memory instead (hflux_wall).
-    auto load_plane = [&](int m, int po, int qo, int mo) {
-        const Slot s = slot(po);
+    auto convert = [&](int m, int s, int po, int mo) {
+        const Slot sl = slot(po);
         R *MU = smu(mo), *PR = sMP + mo + NB;
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
@@ -566,12 +705,15 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
         for (int l = 0; l < NL; l++) {
             if (lp[l] < 0) continue;
             const int p = lp[l] & 0xffff;
-            const long long off = (long long)m * plane + lo[l];
+            const bool r1 = (lp[l] & 0x10000) != 0;
             double q[5];
+            if (!TMA) {
+                const long long off = (long long)m * plane + lo[l];
 #pragma unroll
-            for (int v = 0; v < 5; v++) {
-                q[v] = ldq(qin() + v * vol + off);
-                sq(qo, v)[p] = (R)q[v];
+                for (int v = 0; v < 5; v++) {
+                    q[v] = ldq_c<PERSIST>(qin() + v * vol + off);
+                    sq(s, v)[p] = (R)q[v];
+                }
             }
             double u, vv, w, T, pr;
             R mu;
@@ -585,16 +727,22 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 pr = W[6 * plane + wo];
                 mu = (R)W[7 * plane + wo];
             } else {
+                if (TMA) {
+#pragma unroll
+                    for (int v = 0; v < 5; v++) q[v] = (double)sq(s, v)[p];
+                }
                 prims_from_q(P, q, u, vv, w, T);
                 pr = (q[0] * T) * P.inv_gM2;
-                mu = (lp[l] & 0x10000) ? mu_of<R>(T) : R(0);
+                mu = r1 ? mu_of<R>(T) : R(0);
             }
-            ((R *)s.U)[p] = (R)u;
-            ((R *)s.V)[p] = (R)vv;
-            ((R *)s.W)[p] = (R)w;
-            ((R *)s.T)[p] = (R)T;
-            MU[p] = mu;
-            if (S::p_ring) PR[p] = (R)pr;
+            ((R *)sl.U)[p] = (R)u;
+            ((R *)sl.V)[p] = (R)vv;
+            ((R *)sl.W)[p] = (R)w;
+            ((R *)sl.T)[p] = (R)T;
+            if (r1) {
+                MU[p] = mu;
+                if (S::p_ring) PR[p] = (R)pr;
+            }
         }
     };
 
@@ -602,7 +750,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
     auto center = [&](int m, double q[5], double &u, double &v, double &w, double &T) {
         const long long off = (long long)m * plane + colo;
 #pragma unroll
-        for (int c = 0; c < 5; c++) q[c] = ldq(qin() + c * vol + off);
+        for (int c = 0; c < 5; c++) q[c] = ldq_c<PERSIST>(qin() + c * vol + off);
         if (m == 1 || m == n3) {
             const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane + colo;
             u = W[1 * plane]; v = W[2 * plane]; w = W[3 * plane]; T = W[5 * plane];
@@ -611,12 +759,13 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
         }
     };
 
-    // hD at the own column of interior plane m (in ring); dz from (m-1, m+1) values
-    auto hflux = [&](int m, int po, int mo, int qo, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
-        const Slot s = slot(po);
+    // hD at the own column of interior plane m (prims at po, (mu,p) at mo, Q
+    // slot s); dz from (m-1, m+1) values
+    auto hflux = [&](int m, int po, int mo, int s, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
+        const Slot sl = slot(po);
         const R sc = ktab<R>(P, 0, m);
-        visc_fz<BX>(C, s, smu(mo)[bc], pres_at(C, s, spr(mo, qo), bc), bc, (up - um) * sc, (vp - vm) * sc, (wp_ - wm) * sc,
-                    (Tp - Tm) * sc, h);
+        visc_fz<BX>(C, sl, smu(mo)[bc], pres_at(C, sl, spr(mo, s), bc), bc, (up - um) * sc, (vp - vm) * sc,
+                    (wp_ - wm) * sc, (Tp - Tm) * sc, h);
     };
     // hD at the own column of wall plane m, from the wall's own values in
     // memory, in double; one-sided dz against the interior neighbour values
@@ -636,14 +785,44 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
         visc_fz_vals(P.cd, ux, vy, wx, wy, u0, v0, w0, W[7 * plane], W[6 * plane], uz, vz, wz, Tz, h);
     };
 
-    // ---------------- prologue: planes kb-1 and kb, hD(kb-1), hD(kb)
+    // halo-flux lanes: fD of the two x-halo columns on lanes 0..2TJ-1 of warp
+    // 0, gD of the two y-halo rows on lanes 32..32+2TI-1.  Each owns one halo
+    // point for the whole march and keeps that point's plane t-1 values (u or
+    // v, and w) in sH[.][tid].  hbox: the point's box index.
+    const bool hx_lane = tid < 2 * TJ;
+    const bool hy_lane = tid >= 32 && tid < 32 + 2 * TI;
+    auto hbox = [&]() -> int {
+        if (hx_lane) {
+            const int side = tid / TJ, r = tid - side * TJ;
+            return (r + 2) * BX + (side ? TI + 2 : 1);
+        }
+        const int h = tid - 32, side = h / TI, cc = h - side * TI;
+        return (side ? TJ + 2 : 1) * BX + cc + 2;
+    };
+    // the halo lane's values (u or v, w) in ring slot sl, kept as plane t-1
+    auto keep_halo = [&](const Slot &sl) {
+        if (hx_lane || hy_lane) {
+            const int b = hbox();
+            sH[tid] = hx_lane ? sl.U[b] : sl.V[b];
+            sH[S::NHL + tid] = sl.W[b];
+        }
+    };
+
+    // ---------------- prologue: planes kb-1 (Q slot 0, prims at pP) and kb
+    // (Q slot 1, prims at pZ); hD(kb-1), hD(kb); plane kb+1 starts its way in
+    issue(kb - 1, 0);
+    issue(kb, 1);
+    issue(kb + 1, 2);   // kb+1 <= ke+1 <= nP3
+    bool bad = !wait_slot(0);
+    convert(kb - 1, 0, pP, mP);
+    bad = !wait_slot(1) || bad;
+    convert(kb, 1, pZ, mZ);
+    if (__syncthreads_or(bad)) { give_up(); return; }
+
     R qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
-    R wm2 = R(0);
-    load_plane(kb - 1, oM, qP, mP);
-    load_plane(kb, oZ, qZ, mZ);
-    __syncthreads();
+    R wm2 = R(0), um1 = R(0), vm1 = R(0), wm1 = R(0);   // own column: w at t-2; u, v, w at t-1
     {
-        const Slot sA = slot(oM), sB = slot(oZ);
+        const Slot sA = slot(pP), sB = slot(pZ);
         if (col_ok) {
             // hD(kb-1)
             if (kb - 1 == 1) {
@@ -654,13 +833,13 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
             } else {
                 double q[5], u, v, w, T;
                 center(kb - 2, q, u, v, w, T);
-                hflux(kb - 1, oM, mP, qP, (R)u, (R)v, (R)w, (R)T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
+                hflux(kb - 1, pP, mP, 0, (R)u, (R)v, (R)w, (R)T, sB.U[bc], sB.V[bc], sB.W[bc], sB.T[bc], hm1);
             }
             // hD(kb)
             {
                 double q[5], u, v, w, T;
                 center(kb + 1, q, u, v, w, T);
-                hflux(kb, oZ, mZ, qZ, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], (R)u, (R)v, (R)w, (R)T, h0);
+                hflux(kb, pZ, mZ, 1, sA.U[bc], sA.V[bc], sA.W[bc], sA.T[bc], (R)u, (R)v, (R)w, (R)T, h0);
             }
             if (kb - 2 >= 1) {
                 double q[5], u, v, w, T;
@@ -678,17 +857,21 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 for (int c = 0; c < 4; c++) P.hwt[c * plane + colo] = h[c];
             }
 #pragma unroll
-            for (int c = 0; c < 5; c++) qm1[c] = sq(qP, c)[bc];
+            for (int c = 0; c < 5; c++) qm1[c] = sq(0, c)[bc];
+            um1 = sA.U[bc]; vm1 = sA.V[bc]; wm1 = sA.W[bc];
         } else {
 #pragma unroll
             for (int c = 0; c < 5; c++) qm1[c] = R(0);
         }
+        keep_halo(sA);
     }
     __syncthreads();
 
     for (int t = kb; t <= ke; t++) {
-        // ---------- A: plane t+1 into the ring; own column of t+2 (and, with
-        // float rings, the own point's RK base starts its way into shared memory)
+        // ---------- A: plane t+2's box starts its way in (converted at the next
+        // plane); own column of t+2; (float rings: the own point's RK base
+        // starts its way into shared memory); plane t+1's box is converted
+        if (t < ke) issue(t + 2, iN);
         if (S::prefetch_base) {
             if (P.rk_mode != 0 && out_ok) {
                 const double *src = P.qbase + (long long)t * plane + colo;
@@ -697,7 +880,6 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
             }
             cp_async_commit();
         }
-        load_plane(t + 1, oP, qP, mP);
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
         if (col_ok && t + 2 <= n3) {
             double q[5], u, v, w, T;
@@ -706,44 +888,46 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
             for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
-        __syncthreads();
+        bad = !wait_slot(iP);
+        convert(t + 1, iP, pP, mP);
+        if (__syncthreads_or(bad)) { give_up(); return; }
 
         // ---------- C: viscous flux vectors
-        const Slot s0 = slot(oZ), sm = slot(oM), sp = slot(oP);
+        const Slot s0 = slot(pZ), sp = slot(pP);
         R hp1[4] = {0, 0, 0, 0};
         {
             const R czt = ktab<R>(P, 0, t);
-            const R *MU = smu(mZ), *PR = spr(mZ, qZ);
+            const R *MU = smu(mZ), *PR = spr(mZ, iZ);
             if (col_ok) {
                 if (t + 1 != n3)
-                    hflux(t + 1, oP, mP, qP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+                    hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 R f[4], g[4];
-                visc_fxy<BX>(C, s0, sm, sp, MU, PR, bc, czt, f, g);
+                visc_fxy<BX>(C, s0, um1, vm1, wm1, sp, MU, PR, bc, czt, f, g);
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
                     sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
                     sG[(c * (TJ + 2) + ty + 1) * TI + tx] = g[c];
                 }
             }
-            // halo fluxes on dedicated lanes: fD of the two x-halo columns on
-            // lanes 0..2TJ-1 of warp 0, gD of the two y-halo rows on warps 1..
-            if (tid < 2 * TJ) {
+            if (hx_lane) {
                 const int side = tid / TJ, r = tid - side * TJ;
                 const int ci = side ? i0 + TI : i0 - 1, cj = j0 + r;
                 if (ci <= n1 && cj <= n2) {
                     R f[4];
-                    visc_fx<BX>(C, s0, sm, sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1), czt, f);
+                    visc_fx<BX>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1),
+                                czt, f);
 #pragma unroll
-                    for (int c = 0; c < 4; c++) sF[(c * TJ + r) * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
+                    for (int c = 0; c < 4; c++) sF[c * S::NFX + r * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
                 }
-            } else if (tid >= 32 && tid < 32 + 2 * TI) {
+            } else if (hy_lane) {
                 const int h = tid - 32, side = h / TI, cc = h - side * TI;
                 const int ci = i0 + cc, cj = side ? j0 + TJ : j0 - 1;
                 if (ci <= n1 && cj <= n2) {
                     R g[4];
-                    visc_fy<BX>(C, s0, sm, sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2, czt, g);
+                    visc_fy<BX>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2,
+                                czt, g);
 #pragma unroll
-                    for (int c = 0; c < 4; c++) sG[(c * (TJ + 2) + (side ? TJ + 1 : 0)) * TI + cc] = g[c];
+                    for (int c = 0; c < 4; c++) sG[c * S::NGY + (side ? TJ + 1 : 0) * TI + cc] = g[c];
                 }
             }
         }
@@ -752,8 +936,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
         // ---------- E: fluxes, source, RK update
         R q0[5];
 #pragma unroll
-        for (int c = 0; c < 5; c++) q0[c] = sq(qZ, c)[bc];
-        const R wm1 = sm.W[bc];
+        for (int c = 0; c < 5; c++) q0[c] = sq(iZ, c)[bc];
         if (out_ok) {
             R Fs[5];   // sum of the flux derivatives
             const R mu0 = smu(mZ)[bc];
@@ -766,7 +949,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 R F1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const R *Q = sq(qZ, c);
+                    const R *Q = sq(iZ, c);
                     F1[c] = wsum(w, Q[bc - 2], Q[bc - 1], Q[bc], Q[bc + 1], Q[bc + 2]);
                 }
                 Fs[0] = F1[0];  // F2 of continuity is zero
@@ -786,7 +969,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 R G1[5];
 #pragma unroll
                 for (int c = 0; c < 5; c++) {
-                    const R *Q = sq(qZ, c);
+                    const R *Q = sq(iZ, c);
                     G1[c] = wsum(w, Q[bc - 2 * BX], Q[bc - BX], Q[bc], Q[bc + BX], Q[bc + 2 * BX]);
                 }
                 Fs[0] = Fs[0] + G1[0];
@@ -809,11 +992,11 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                     inv_weights(wm2, wm1, w0, wp1, wp2, qk, ktab<R>(P, 1, t), ktab<R>(P, 2, t), w);
                 }
                 const R czt = ktab<R>(P, 0, t);
-                Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(qP, 0)[bc], qp2[0]);
+                Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const R H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(qP, c)[bc], qp2[c]);
+                    const R H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(iP, c)[bc], qp2[c]);
                     const R hp = top ? (R)P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
                     const R H2 = (hp - hm1[c - 1]) * czt;
                     Fs[c] = (Fs[c] + H1) + H2;
@@ -832,7 +1015,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
             Rd[1] = src2 - (double)Fs[1];
             Rd[2] = -(double)Fs[2];
             Rd[3] = -(double)Fs[3];
-            if (BUOY) {
+            if (buoy) {
                 // buoyancy on the wall-normal momentum and its work on the energy
                 const double bq = P.ri * ((double)q0[0] * ((double)s0.T[bc] - P.tref));
                 Rd[3] = bq - (double)Fs[3];
@@ -847,7 +1030,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
             } else {
                 const long long off = (long long)t * plane + colo;
 #pragma unroll
-                for (int c = 0; c < 5; c++) qs[c] = ldq(qin() + c * vol + off);
+                for (int c = 0; c < 5; c++) qs[c] = ldq_c<PERSIST>(qin() + c * vol + off);
             }
             double qn[5];
             double qb[5] = {0, 0, 0, 0, 0};
@@ -859,7 +1042,7 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 } else {
                     const long long off = (long long)t * plane + colo;
 #pragma unroll
-                    for (int c = 0; c < 5; c++) qb[c] = __ldg(P.qbase + c * vol + off);
+                    for (int c = 0; c < 5; c++) qb[c] = ldq_c<PERSIST>(P.qbase + c * vol + off);
                 }
             }
             if (P.rk_mode == 0) {
@@ -894,27 +1077,38 @@ __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb) k_stage(c
                 if (!fin) flag_nonfinite(P.status, i, j, t);
             }
         }
-        // ---------- F: rotate the column registers
+        // ---------- F: plane t becomes t-1; rotate the rings
 #pragma unroll
         for (int c = 0; c < 5; c++) {
             qm2[c] = qm1[c];
             qm1[c] = q0[c];
         }
         wm2 = wm1;
+        um1 = s0.U[bc]; vm1 = s0.V[bc]; wm1 = s0.W[bc];
+        keep_halo(s0);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             hm1[c] = h0[c];
             h0[c] = hp1[c];
         }
         {
-            const int o = oM;
-            oM = oZ; oZ = oP; oP = o;
-            int x = qZ; qZ = qP; qP = x;
+            const int o = iZ;
+            iZ = iP; iP = iN; iN = o;
+            int x = pZ; pZ = pP; pP = x;
             x = mZ; mZ = mP; mP = x;
         }
         __syncthreads();
     }
     if (S::prefetch_base) cp_async_wait<0>();
+}
+
+template <int TI, int TJ, typename QI, typename QO, typename R, bool BUOY>
+__global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb)
+    k_stage(const KParams P, const __grid_constant__ CUtensorMap tmq)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    stage_body<TI, TJ, QI, QO, R, BUOY ? 1 : 0, false>(P, &tmq, blockIdx.x, blockIdx.y, blockIdx.z, threadIdx.x,
+                                                          threadIdx.y, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -976,23 +1170,26 @@ __device__ void wall_point(const KParams &P, int wall, int i, int j, double &u, 
 
 // QT: storage type of the stage output the wall BC reads (the planes next to the wall)
 constexpr int kWallBX = 32, kWallBY = 8;
+constexpr int kWallHX = kWallBX + 2, kWallHY = kWallBY + 2;
+using WallStage = double[2][6][kWallHY][kWallHX];
+
+// One block's work of the wall kernel: block (bx, by) of wall `wall`,
+// thread (tx, ty), near-wall staging area sp.
 template <typename QT>
-__global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
+__device__ __forceinline__ void wall_body(const KParams &P, int bx_, int by_, int wall, int tx, int ty, WallStage &sp)
 {
     const QT *qo = static_cast<const QT *>(P.qout);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int wall = blockIdx.z;
+    const int i = bx_ * kWallBX + tx;
+    const int j = by_ * kWallBY + ty;
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
     const long long plane = P.plane, vol = P.vol;
     // primitives of the two planes next to the wall on the block's (i,j) tile
     // plus a 1-point halo, each computed once: [plane][r,u,v,w,p,mu][by][bx]
-    constexpr int HX = kWallBX + 2, HY = kWallBY + 2;
-    __shared__ double sp[2][6][HY][HX];
+    constexpr int HX = kWallHX, HY = kWallHY;
     {
         const int k2 = wall == 0 ? 2 : n3 - 1, k3 = wall == 0 ? 3 : n3 - 2;
-        const int i0 = blockIdx.x * blockDim.x - 1, j0 = blockIdx.y * blockDim.y - 1;
-        for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < 2 * HX * HY; e += blockDim.x * blockDim.y) {
+        const int i0 = bx_ * kWallBX - 1, j0 = by_ * kWallBY - 1;
+        for (int e = ty * kWallBX + tx; e < 2 * HX * HY; e += kWallBX * kWallBY) {
             const int pl = e / (HX * HY), r0 = e - pl * HX * HY, by = r0 / HX, bx = r0 - by * HX;
             const int ii = i0 + bx, jj = j0 + by;
             if (ii < 1 || ii > n1 || jj < 1 || jj > n2) continue;
@@ -1035,7 +1232,7 @@ __global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
         auto prim = [&](int ii, int jj, int kk, double &r, double &u, double &v, double &w, double &T,
                         double &p, double &mu) {
             const int pl = kk == k2 ? 0 : 1;
-            const int bx = ii - (int)(blockIdx.x * blockDim.x) + 1, by = jj - (int)(blockIdx.y * blockDim.y) + 1;
+            const int bx = ii - bx_ * kWallBX + 1, by = jj - by_ * kWallBY + 1;
             r = sp[pl][0][by][bx];
             u = sp[pl][1][by][bx];
             v = sp[pl][2][by][bx];
@@ -1095,6 +1292,13 @@ __global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
     }
 }
 
+template <typename QT>
+__global__ void __launch_bounds__(kWallBX * kWallBY) k_wall(const KParams P)
+{
+    __shared__ double sp[2][6][kWallHY][kWallHX];
+    wall_body<QT>(P, blockIdx.x, blockIdx.y, blockIdx.z, threadIdx.x, threadIdx.y, sp);
+}
+
 // ---------------------------------------------------------------------------
 // var(i,j,k,1:7) as the reference holds it after a stage (used by the
 // statistics, the blow-up scan and downloads).
@@ -1142,13 +1346,13 @@ __device__ __forceinline__ double warp_sum(double v)
 // pb = n3, n3+1: the wall-shear sum of the bottom, top wall) into
 // part[(pb*S + sub)*23 + c].  Pass 2 adds the S partial sums in a fixed
 // order: the result is deterministic.
-__global__ void __launch_bounds__(kStatThreads, 3) k_stats_part(const KParams P, const double *q, int do_moments,
-                                                             int do_tau, int S, double *part)
+using StatRed = double[kStatThreads / 32][23];
+__device__ __forceinline__ void stats_part_body(const KParams &P, const double *q, int do_moments, int do_tau, int S,
+                                                double *part, int blk, int tid, StatRed &red)
 {
-    __shared__ double red[kStatThreads / 32][23];
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
-    const int pb = blockIdx.x / S, sub = blockIdx.x - pb * S;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pb = blk / S, sub = blk - pb * S;
+    const int lane = tid & 31, warp = tid >> 5;
     if (frozen(P.status, kstep(P) + 1)) return;
     double *out = part + ((size_t)pb * S + sub) * 23;
     if (pb < n3) {
@@ -1219,13 +1423,20 @@ __global__ void __launch_bounds__(kStatThreads, 3) k_stats_part(const KParams P,
     }
 }
 
+__global__ void __launch_bounds__(kStatThreads, 3) k_stats_part(const KParams P, const double *q, int do_moments,
+                                                             int do_tau, int S, double *part)
+{
+    __shared__ double red[kStatThreads / 32][23];
+    stats_part_body(P, q, do_moments, do_tau, S, part, blockIdx.x, threadIdx.x, red);
+}
+
 // Pass 2: one warp per plane / wall adds the S partial sums in order and
 // writes stat1Spc, stat2Spc, corrSpc (divided by nP1*nP2) and tauL, tauU
 // (divided by (nP1-2)*(nP2-2)); with time averaging on, also adds them into tacc.
-__global__ void k_stats_fin(const KParams P, int do_moments, int do_tau, int S, const double *part)
+__device__ __forceinline__ void stats_fin_body(const KParams &P, int do_moments, int do_tau, int S, const double *part,
+                                               int pb, int c)
 {
     const int n1 = P.n1, n2 = P.n2, n3 = P.n3;
-    const int pb = blockIdx.x, c = threadIdx.x;
     if (frozen(P.status, kstep(P) + 1)) return;
     const double *in = part + (size_t)pb * S * 23;
     if (pb < n3) {
@@ -1249,6 +1460,11 @@ __global__ void k_stats_fin(const KParams P, int do_moments, int do_tau, int S, 
     const double val = s / (double)((n1 - 2) * (n2 - 2));
     P.stat[(size_t)23 * n3 + wall] = val;
     if (P.acc_on) P.tacc[(size_t)23 * n3 + wall] += val;
+}
+
+__global__ void k_stats_fin(const KParams P, int do_moments, int do_tau, int S, const double *part)
+{
+    stats_fin_body(P, do_moments, do_tau, S, part, blockIdx.x, threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1723,6 +1939,172 @@ __global__ void k_selftest_pow07(const double *T, double *mine, double *libm, lo
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         mine[i] = pow07(T[i]);
         libm[i] = pow(T[i], 0.7);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent ensemble kernel.
+//
+// One launch runs a block of L time steps of every member of an ensemble.  The
+// host lays the work out as phases -- for each member and step: the clock
+// advance, then per RK stage the stage kernel's CTAs and the wall kernel's
+// blocks, then on statistics steps the two statistics passes -- each phase a
+// number of units (one unit = one CTA's work of the kernel it replaces), and
+// lists all units of all members in one work list, members interleaved.  CTAs
+// take units from the list in order through an atomic counter.  A unit may
+// start once its member has completed every unit of its earlier phases: the
+// member's completion counter reaches the phase's `need`.  Units are taken in
+// list order and a unit only waits for units earlier in the list, which
+// running CTAs hold, so the launch always progresses; each wait is still
+// bounded (about a second), after which the CTA records the error and stops.
+// Every member's arithmetic is the stand-alone kernels' code, so its results
+// are bit for bit those of chan_step.
+enum PKind { kPClock = 0, kPStage = 1, kPWall = 2, kPStatsPart = 3, kPStatsFin = 4 };
+
+struct PPhase {
+    int member;
+    int kind;            // PKind
+    int variant;         // stage: 0 FP64, 1..3 mixed first / middle / last; wall: 0 double, 1 float state
+    int tile;            // stage: CHAN_TILE_32x8 (0) or CHAN_TILE_16x16 (2)
+    int nx, ny;          // stage: tiles in x, y; wall: blocks in x, y; stats: blocks per plane (S)
+    int kp;              // index of the member's KParams record for this phase
+    int units;
+    unsigned long long need;    // member's completed units before this phase may start
+    double dt;                  // clock advance
+    const CUtensorMap *tm;      // stage: tensor map of the input buffer
+    const double *q;            // statistics: the state buffer
+    double *part;               // statistics: partial sums
+};
+
+struct PItem {
+    int phase;
+    int unit;
+};
+
+struct PPlan {
+    const PPhase *phases;
+    const PItem *items;
+    long long nitems;
+    const KParams *kps;
+    unsigned long long *done;   // [members] completed units
+    unsigned long long *next;   // work-list position
+    int *err;                   // 1: a dependency wait gave up
+    DevClock *clk;              // [members]
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr unsigned long long kDepWaitNs = 1000000000ull;
+
+template <int TI, int TJ, typename QI, typename QO, typename R>
+__device__ __forceinline__ void pstage(const PPhase &F, const KParams &P, int unit, int tid, unsigned char *smem)
+{
+    const int bx = unit % F.nx, r = unit / F.nx, by = r % F.ny, bz = r / F.ny;
+    stage_body<TI, TJ, QI, QO, R, 2, true>(P, F.tm, bx, by, bz, tid % TI, tid / TI, smem);
+}
+
+template <bool MIXED>
+struct PersistShape {
+    // dynamic shared memory: the largest unit's, plus the work-item slot
+    static constexpr size_t st = MIXED ? (StageShape<32, 8, float>::bytes > StageShape<16, 16, float>::bytes
+                                               ? StageShape<32, 8, float>::bytes
+                                               : StageShape<16, 16, float>::bytes)
+                                       : (StageShape<32, 8, double>::bytes > StageShape<16, 16, double>::bytes
+                                              ? StageShape<32, 8, double>::bytes
+                                              : StageShape<16, 16, double>::bytes);
+    static constexpr size_t wall = sizeof(double) * 2 * 6 * kWallHY * kWallHX;
+    static constexpr size_t body = ((st > wall ? st : wall) + 127) / 128 * 128;
+    static constexpr size_t bytes = body + 128;
+    static constexpr int minb = MIXED ? 3 : 2;
+};
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(const PPlan plan)
+{
+    using PS = PersistShape<MIXED>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    long long *s_item = reinterpret_cast<long long *>(smem_raw + PS::body);
+    int *s_ok = reinterpret_cast<int *>(s_item + 1);
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) {
+            long long it = (long long)atomicAdd(plan.next, 1ull);
+            if (it < plan.nitems && *(volatile int *)plan.err) it = plan.nitems;   // after an error: stop
+            int ok = 1;
+            if (it < plan.nitems) {
+                const PPhase &F = plan.phases[plan.items[it].phase];
+                const unsigned long long *d = plan.done + F.member;
+                if (ld_acquire_u64(d) < F.need) {
+                    const unsigned long long t0 = global_ns();
+                    while (ld_acquire_u64(d) < F.need) {
+                        if (global_ns() - t0 > kDepWaitNs) { ok = 0; break; }
+                        __nanosleep(256);
+                    }
+                }
+                if (!ok) atomicExch(plan.err, 1);
+            }
+            *s_item = it;
+            *s_ok = ok;
+        }
+        __syncthreads();
+        const long long it = *s_item;
+        const int ok = *s_ok;
+        __syncthreads();
+        if (it >= plan.nitems || !ok) break;
+        const PItem I = plan.items[it];
+        const PPhase &F = plan.phases[I.phase];
+        const KParams &P = plan.kps[F.kp];
+        switch (F.kind) {
+        case kPClock:
+            if (tid == 0) {
+                DevClock *c = plan.clk + F.member;
+                c->step = c->step + 1;
+                c->time = c->time + F.dt;
+            }
+            break;
+        case kPStage:
+            if (!MIXED) {
+                if (F.tile == 0) pstage<32, 8, double, double, double>(F, P, I.unit, tid, smem_raw);
+                else pstage<16, 16, double, double, double>(F, P, I.unit, tid, smem_raw);
+            } else if (F.tile == 0) {
+                if (F.variant == 1) pstage<32, 8, double, float, float>(F, P, I.unit, tid, smem_raw);
+                else if (F.variant == 2) pstage<32, 8, float, float, float>(F, P, I.unit, tid, smem_raw);
+                else pstage<32, 8, float, double, float>(F, P, I.unit, tid, smem_raw);
+            } else {
+                if (F.variant == 1) pstage<16, 16, double, float, float>(F, P, I.unit, tid, smem_raw);
+                else if (F.variant == 2) pstage<16, 16, float, float, float>(F, P, I.unit, tid, smem_raw);
+                else pstage<16, 16, float, double, float>(F, P, I.unit, tid, smem_raw);
+            }
+            break;
+        case kPWall: {
+            const int bx = I.unit % F.nx, r = I.unit / F.nx, by = r % F.ny, wall = r / F.ny;
+            WallStage &sp = *reinterpret_cast<WallStage *>(smem_raw);
+            if (F.variant == 0) wall_body<double>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
+            else wall_body<float>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
+            break;
+        }
+        case kPStatsPart:
+            stats_part_body(P, F.q, 1, 1, F.nx, F.part, I.unit, tid, *reinterpret_cast<StatRed *>(smem_raw));
+            break;
+        case kPStatsFin: {
+            const int pb = I.unit * 8 + (tid >> 5);
+            if (pb < P.n3 + 2) stats_fin_body(P, 1, 1, F.nx, F.part, pb, tid & 31);
+            break;
+        }
+        default:
+            break;
+        }
+        // the unit's writes (all threads) before its completion is counted
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(plan.done + F.member, 1ull);
+        }
     }
 }
 

@@ -7,6 +7,8 @@
 #include "chan_internal.h"
 #include "chan_kernels.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -19,7 +21,7 @@ namespace {
 // Stage-kernel tile shapes: TI columns in x (one warp row) by TJ rows in y.
 // Each shape has the plain FP64 kernel and the three mixed-precision stage
 // kernels, without and with the buoyancy term.
-using StageFn = void (*)(const chan::KParams);
+using StageFn = void (*)(const chan::KParams, const CUtensorMap);
 struct StageSet {
     int ti, tj;
     StageFn k[2][4];   // [buoyancy][0 FP64, 1 mixed first stage, 2 mixed middle, 3 mixed last]
@@ -81,6 +83,10 @@ struct chan_ctx {
     int n1 = 0, n2 = 0, n3 = 0, px = 0, NJ = 0;
     long long plane = 0, vol = 0;
     int tile = CHAN_TILE_32x8, ntx = 0, nty = 0, nchunks = 1, kchunk = 1;   // stage-kernel launch shape
+    // tensor maps of the stage kernel's box copies, per tile shape: the three
+    // FP64 state buffers, or the two float stage buffers (mixed precision)
+    CUtensorMap tmd[CHAN_NTILES][3];
+    CUtensorMap tmf[CHAN_NTILES][2];
     int nstage = 2;
     int cur = 0;             // buffer holding the latest state
     bool uploaded = false;
@@ -198,6 +204,56 @@ void wall_coeffs(const double *x3, int n3, double out[14])
     out[11] = one / t;
     out[12] = dz1;
     out[13] = dzN;
+}
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (no -lcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+// tensor map of one state buffer [5][nP3+2][nP2+2][px] for the stage
+// kernel's box copies: box (TI+4) x (TJ+4) x 1 plane x 5 variables, no
+// swizzle, points beyond nP1+1 / nP2+1 read as zero.  A box's x origin is a
+// multiple of TI (16 or 32 elements), so every copy starts on a 16-byte
+// boundary; the rows, planes and variables are px, plane and vol elements
+// apart (multiples of 8 elements).
+int make_state_map(chan_ctx *c, CUtensorMap *m, void *base, bool is_float, int ti, int tj)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) { c->err = "cuTensorMapEncodeTiled is not available"; return CHAN_ECUDA; }
+    const cuuint64_t es = is_float ? 4 : 8;
+    const cuuint64_t dims[4] = {(cuuint64_t)c->n1 + 2, (cuuint64_t)c->n2 + 2, (cuuint64_t)c->n3 + 2, 5};
+    const cuuint64_t strides[3] = {(cuuint64_t)c->px * es, (cuuint64_t)c->plane * es, (cuuint64_t)c->vol * es};
+    const cuuint32_t box[4] = {(cuuint32_t)ti + 4, (cuuint32_t)tj + 4, 1, 5};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(m, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base,
+                           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        c->err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return CHAN_ECUDA;
+    }
+    return CHAN_OK;
+}
+
+// the tensor map of the current stage's input buffer (any map when that
+// stage loads its boxes with per-thread loads)
+const CUtensorMap &stage_map(const chan_ctx *c)
+{
+    for (int b = 0; b < 3; b++)
+        if (!c->mixed && c->kp.qin == (const void *)c->q[b]) return c->tmd[c->tile][b];
+    for (int b = 0; b < 2; b++)
+        if (c->mixed && c->kp.qin == (const void *)c->qf[b]) return c->tmf[c->tile][b];
+    return c->tmd[c->tile][0];
 }
 
 void set_stage(chan_ctx *c, int iter)
@@ -324,7 +380,8 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
         const StageSet &ss = kStageSets[c->tile];
         dim3 grid(c->ntx, c->nty, c->nchunks), block(ss.ti, ss.tj);
         const int v = !c->mixed ? 0 : (iter == 1 ? 1 : (last ? 3 : 2));
-        ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(c->kp);
+        ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(c->kp,
+                                                                                               stage_map(c));
     }
     if (c->closure_on) {
         chan::k_sgs_apply<<<1184, 256, 0, c->stream>>>(c->kp, (double *)c->kp.qout, c->sgsS, c->kp.rk_cdt);
@@ -440,6 +497,11 @@ int read_status(chan_ctx *c, int32_t *ijk)
     if (s.nonfinite) {
         if (ijk) { ijk[0] = s.nf_ijk[0]; ijk[1] = s.nf_ijk[1]; ijk[2] = s.nf_ijk[2]; }
         return CHAN_NONFINITE;
+    }
+    if (s.stall) {
+        c->err = s.stall == 1 ? "stage kernel: a bulk box copy did not complete within its time limit"
+                              : "stage kernel: shared-memory staging area not 128-byte aligned";
+        return CHAN_ECUDA;
     }
     if (ijk) ijk[0] = ijk[1] = ijk[2] = 0;
     c->sync_nstep = c->nstep;
@@ -712,6 +774,15 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
                 e = cudaFuncSetAttribute((const void *)ss.k[b][v], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(v == 0 ? ss.smem : ss.smemf));
     if (e != cudaSuccess) { fail(nullptr, "cudaFuncSetAttribute", e); chan_free(c); return CHAN_ECUDA; }
+    memset(c->tmd, 0, sizeof(c->tmd));
+    memset(c->tmf, 0, sizeof(c->tmf));
+    for (int t = 0; t < CHAN_NTILES; t++) {
+        const int ti = kStageSets[t].ti, tj = kStageSets[t].tj;
+        for (int b = 0; b < 3 && !c->mixed; b++)
+            if ((r = make_state_map(c, &c->tmd[t][b], c->q[b], false, ti, tj))) { g_init_error = c->err; chan_free(c); return r; }
+        for (int b = 0; b < 2 && c->mixed; b++)
+            if ((r = make_state_map(c, &c->tmf[t][b], c->qf[b], true, ti, tj))) { g_init_error = c->err; chan_free(c); return r; }
+    }
     if (set_launch(c, CHAN_TILE_32x8, 0) != CHAN_OK) { g_init_error = c->err; chan_free(c); return CHAN_ECUDA; }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
@@ -1503,6 +1574,20 @@ struct chan_ensemble {
     long long replays = 0, captures = 0;
     double last_ms = 0.0;             // device time of the last call's graph replays (CUDA events)
     std::string err;
+    // persistent mode: one persistent kernel per block of L steps (k_ensemble)
+    int mode = CHAN_ENSEMBLE_PERSISTENT;   // requested mode
+    bool persistent = false;               // the captured graph holds the persistent kernel
+    std::string fallback;                  // why the requested persistent mode fell back
+    chan::PPhase *dph = nullptr;
+    chan::PItem *ditems = nullptr;
+    chan::KParams *dkps = nullptr;
+    CUtensorMap *dmaps = nullptr;
+    unsigned long long *dcnt = nullptr;    // [n] completed units per member, then the work-list position
+    int *derr = nullptr, *herr = nullptr;
+    size_t cap_ph = 0, cap_items = 0, cap_kps = 0, cap_maps = 0;
+    long long nitems = 0;
+    int pgrid = 0;
+    bool stall_test = false;               // host-side fault injection for tests
 };
 
 namespace {
@@ -1551,10 +1636,180 @@ int members_wait_origin(chan_ensemble *e)
     return CHAN_OK;
 }
 
+// (re)allocate a device array for n elements when it holds fewer
+template <typename T>
+cudaError_t ensure_dev(T **p, size_t *cap, size_t n)
+{
+    if (*p && *cap >= n) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t r = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (r == cudaSuccess) *cap = n;
+    return r;
+}
+
+// why the members cannot run in the persistent kernel ("" if they can)
+std::string persistent_blocker(const chan_ensemble *e)
+{
+    const bool mixed = e->m[0]->mixed;
+    for (chan_ctx *c : e->m) {
+        if (c->mixed != mixed) return "members of both precisions";
+        if (c->closure_on) return "a member runs with the learned closure";
+        if (c->tile != CHAN_TILE_32x8 && c->tile != CHAN_TILE_16x16) return "a member uses the 32x4 tile";
+    }
+    return "";
+}
+
+// The work list of one block of L steps of every member for k_ensemble, its
+// upload, and the graph of one block: reset the counters, one launch.
+int build_persistent(chan_ensemble *e)
+{
+    const size_t n = e->m.size();
+    const bool mixed = e->m[0]->mixed;
+    std::vector<chan::KParams> kps;
+    std::vector<CUtensorMap> maps;
+    std::vector<std::vector<chan::PPhase>> per(n);
+    for (size_t i = 0; i < n; i++) {
+        chan_ctx *c = e->m[i];
+        const int kp0 = (int)kps.size();
+        for (int it = 1; it <= c->nstage; it++) {
+            set_stage(c, it);
+            chan::KParams k = c->kp;
+            k.check = it == c->nstage ? 1 : 0;
+            k.clk = e->dclk + i;
+            kps.push_back(k);
+            maps.push_back(stage_map(c));
+        }
+        unsigned long long need = 0;
+        auto add = [&](chan::PPhase ph) {
+            ph.member = (int)i;
+            ph.need = need;
+            need += (unsigned long long)ph.units;
+            per[i].push_back(ph);
+        };
+        for (int s = 0; s < e->L; s++) {
+            chan::PPhase ck{};
+            ck.kind = chan::kPClock; ck.units = 1; ck.kp = kp0; ck.dt = c->p.dt;
+            add(ck);
+            for (int it = 1; it <= c->nstage; it++) {
+                const bool last = it == c->nstage;
+                chan::PPhase st{};
+                st.kind = chan::kPStage;
+                st.variant = !c->mixed ? 0 : (it == 1 ? 1 : (last ? 3 : 2));
+                st.tile = c->tile;
+                st.nx = c->ntx; st.ny = c->nty;
+                st.units = c->ntx * c->nty * c->nchunks;
+                st.kp = kp0 + it - 1;
+                st.tm = nullptr;   // set after upload (index kp0 + it - 1 of the maps)
+                add(st);
+                chan::PPhase w{};
+                w.kind = chan::kPWall;
+                w.variant = (c->mixed && !last) ? 1 : 0;
+                w.nx = (c->n1 + 2 + chan::kWallBX - 1) / chan::kWallBX;
+                w.ny = (c->n2 + 2 + chan::kWallBY - 1) / chan::kWallBY;
+                w.units = w.nx * w.ny * 2;
+                w.kp = kp0 + it - 1;
+                add(w);
+            }
+            if (c->p.istat > 0 && (c->nstep + s + 1) % c->p.istat == 0) {
+                chan::PPhase a{};
+                a.kind = chan::kPStatsPart; a.nx = c->nsplit; a.units = (c->n3 + 2) * c->nsplit;
+                a.kp = kp0 + c->nstage - 1; a.q = c->q[0]; a.part = c->spart;
+                add(a);
+                chan::PPhase b = a;
+                b.kind = chan::kPStatsFin; b.units = (c->n3 + 2 + 7) / 8;
+                add(b);
+            }
+        }
+    }
+    // the phases in one array; the units interleaved member by member, phase by phase
+    std::vector<chan::PPhase> ph;
+    std::vector<chan::PItem> items;
+    std::vector<size_t> first(n);
+    size_t maxp = 0;
+    for (size_t i = 0; i < n; i++) {
+        first[i] = ph.size();
+        ph.insert(ph.end(), per[i].begin(), per[i].end());
+        maxp = std::max(maxp, per[i].size());
+    }
+    for (size_t q = 0; q < maxp; q++)
+        for (size_t i = 0; i < n; i++)
+            if (q < per[i].size())
+                for (int u = 0; u < per[i][q].units; u++) items.push_back({(int)(first[i] + q), u});
+    EK(e, ensure_dev(&e->dmaps, &e->cap_maps, maps.size()));
+    for (auto &f : ph)
+        if (f.kind == chan::kPStage) f.tm = e->dmaps + f.kp;
+    if (e->stall_test && !ph.empty()) {
+        // host-side fault injection: member 0's first stage waits for a unit count never reached
+        for (size_t k = 0; k < per[0].size(); k++)
+            if (ph[first[0] + k].kind == chan::kPStage) { ph[first[0] + k].need = ~0ULL; break; }
+    }
+    EK(e, ensure_dev(&e->dph, &e->cap_ph, ph.size()));
+    EK(e, ensure_dev(&e->ditems, &e->cap_items, items.size()));
+    EK(e, ensure_dev(&e->dkps, &e->cap_kps, kps.size()));
+    if (!e->dcnt) EK(e, cudaMalloc((void **)&e->dcnt, (n + 1) * sizeof(unsigned long long)));
+    if (!e->derr) EK(e, cudaMalloc((void **)&e->derr, sizeof(int)));
+    if (!e->herr) EK(e, cudaMallocHost((void **)&e->herr, sizeof(int)));
+    EK(e, cudaMemcpyAsync(e->dmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, e->origin));
+    EK(e, cudaMemcpyAsync(e->dph, ph.data(), ph.size() * sizeof(chan::PPhase), cudaMemcpyHostToDevice, e->origin));
+    EK(e, cudaMemcpyAsync(e->ditems, items.data(), items.size() * sizeof(chan::PItem), cudaMemcpyHostToDevice,
+                          e->origin));
+    EK(e, cudaMemcpyAsync(e->dkps, kps.data(), kps.size() * sizeof(chan::KParams), cudaMemcpyHostToDevice, e->origin));
+    EK(e, cudaMemsetAsync(e->derr, 0, sizeof(int), e->origin));
+    EK(e, cudaStreamSynchronize(e->origin));   // the host vectors are temporaries
+    e->nitems = (long long)items.size();
+
+    const void *fn = mixed ? (const void *)chan::k_ensemble<true> : (const void *)chan::k_ensemble<false>;
+    const size_t smem = mixed ? chan::PersistShape<true>::bytes : chan::PersistShape<false>::bytes;
+    EK(e, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0, sms = 148;
+    EK(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, smem));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev);
+    e->pgrid = std::max(1, occ) * sms;
+
+    chan::PPlan plan{};
+    plan.phases = e->dph; plan.items = e->ditems; plan.nitems = e->nitems; plan.kps = e->dkps;
+    plan.done = e->dcnt; plan.next = e->dcnt + n; plan.err = e->derr; plan.clk = e->dclk;
+    EK(e, cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+    cudaError_t r = cudaMemsetAsync(e->dcnt, 0, (n + 1) * sizeof(unsigned long long), e->origin);
+    if (r == cudaSuccess) {
+        if (mixed)
+            chan::k_ensemble<true><<<e->pgrid, 256, smem, e->origin>>>(plan);
+        else
+            chan::k_ensemble<false><<<e->pgrid, 256, smem, e->origin>>>(plan);
+        r = cudaGetLastError();
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t re = cudaStreamEndCapture(e->origin, &g);
+    if (r != cudaSuccess) { if (g) cudaGraphDestroy(g); return efail(e, "persistent capture", r); }
+    if (re != cudaSuccess) return efail(e, "cudaStreamEndCapture", re);
+    const cudaError_t ri = cudaGraphInstantiate(&e->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ri != cudaSuccess) { e->exec = nullptr; return efail(e, "cudaGraphInstantiate", ri); }
+    return CHAN_OK;
+}
+
 // capture L steps of every member into one graph (host counters restored)
 int build_graph(chan_ensemble *e)
 {
     if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+    e->persistent = false;
+    e->fallback.clear();
+    if (e->mode == CHAN_ENSEMBLE_PERSISTENT) {
+        e->fallback = persistent_blocker(e);
+        if (e->fallback.empty()) {
+            const int rc = build_persistent(e);
+            if (rc) return rc;
+            for (size_t i = 0; i < e->m.size(); i++) {
+                e->cap_epoch[i] = e->m[i]->epoch;
+                e->cap_phase[i] = member_phase(e->m[i]);
+            }
+            e->persistent = true;
+            e->captures++;
+            return CHAN_OK;
+        }
+    }
     EK(e, cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
     int rc = CHAN_OK;
     cudaError_t r = cudaEventRecord(e->fork, e->origin);
@@ -1710,6 +1965,16 @@ int chan_ensemble_step(chan_ensemble *e, int32_t nsteps, int32_t *status)
     }
     // the pinned clock staging is reused by the next call: it has been read
     EK(e, cudaStreamSynchronize(e->origin));
+    if (timed && e->persistent) {
+        EK(e, cudaMemcpy(e->herr, e->derr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (*e->herr) {
+            e->err = "persistent ensemble kernel: a unit waited more than a second for its member's earlier "
+                     "work and the launch stopped; the members' states are undefined (upload or restore them)";
+            EK(e, cudaMemset(e->derr, 0, sizeof(int)));
+            if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+            return CHAN_ECUDA;
+        }
+    }
     e->last_ms = 0.0;
     if (timed) {
         float ms = 0.f;
@@ -1748,11 +2013,12 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
         nch[i] = c->nchunks;
     }
     // candidate shapes of one member: each tile shape at several k-chunk depths
-    auto candidates = [](const chan_ctx *c) {
+    auto candidates = [e](const chan_ctx *c) {
         std::vector<std::pair<int, int>> v;
         const int nz = c->n3 - 2;
         const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
         for (int t = 0; t < CHAN_NTILES; t++) {
+            if (e->mode == CHAN_ENSEMBLE_PERSISTENT && t == CHAN_TILE_32x4) continue;   // 128-thread CTAs
             int last = -1;
             for (int d : depth) {
                 const int nc = std::max(1, (nz + std::min(d, nz) - 1) / std::min(d, nz));
@@ -1778,6 +2044,7 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
         const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
         for (int t = 0; t < CHAN_NTILES && rc == CHAN_OK; t++)
             for (int d : depth) {
+                if (e->mode == CHAN_ENSEMBLE_PERSISTENT && t == CHAN_TILE_32x4) continue;   // 128-thread CTAs
                 std::vector<int> tt(n, t), cc(n);
                 for (size_t i = 0; i < n; i++) {
                     const int nz = e->m[i]->n3 - 2, dd = std::min(d, nz);
@@ -1836,6 +2103,27 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
     return rc;
 }
 
+int chan_ensemble_set_mode(chan_ensemble *e, int32_t mode)
+{
+    if (!e) return CHAN_EINVAL;
+    if (mode != CHAN_ENSEMBLE_GRAPH && mode != CHAN_ENSEMBLE_PERSISTENT && mode != CHAN_ENSEMBLE_PERSISTENT_STALL_TEST) {
+        e->err = "unknown ensemble mode";
+        return CHAN_EINVAL;
+    }
+    e->stall_test = mode == CHAN_ENSEMBLE_PERSISTENT_STALL_TEST;
+    e->mode = mode == CHAN_ENSEMBLE_GRAPH ? CHAN_ENSEMBLE_GRAPH : CHAN_ENSEMBLE_PERSISTENT;
+    if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+    return CHAN_OK;
+}
+
+int chan_ensemble_get_mode(chan_ensemble *e, int32_t *in_use, const char **fallback_reason)
+{
+    if (!e) return CHAN_EINVAL;
+    if (in_use) *in_use = e->exec ? (e->persistent ? CHAN_ENSEMBLE_PERSISTENT : CHAN_ENSEMBLE_GRAPH) : -1;
+    if (fallback_reason) *fallback_reason = e->fallback.c_str();
+    return CHAN_OK;
+}
+
 int chan_ensemble_counters(chan_ensemble *e, int64_t *replays, int64_t *captures, double *last_ms)
 {
     if (!e) return CHAN_EINVAL;
@@ -1862,6 +2150,13 @@ void chan_ensemble_free(chan_ensemble *e)
     if (e->t1) cudaEventDestroy(e->t1);
     if (e->dclk) cudaFree(e->dclk);
     if (e->hclk) cudaFreeHost(e->hclk);
+    if (e->dph) cudaFree(e->dph);
+    if (e->ditems) cudaFree(e->ditems);
+    if (e->dkps) cudaFree(e->dkps);
+    if (e->dmaps) cudaFree(e->dmaps);
+    if (e->dcnt) cudaFree(e->dcnt);
+    if (e->derr) cudaFree(e->derr);
+    if (e->herr) cudaFreeHost(e->herr);
     if (e->origin) cudaStreamDestroy(e->origin);
     delete e;
 }

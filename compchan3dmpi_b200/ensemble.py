@@ -1,11 +1,15 @@
 """Ensembles of channel cases stepped together on one GPU, and the stratified
 parameter sweep they are built for.
 
-``Ensemble`` wraps chan_ensemble_* (include/chanrhs.h): the members' steps
-are captured into one CUDA graph per block of L steps (L = least common
-multiple of the members' istat) and replayed; every member's kernels run
-concurrently on its own stream.  Results are bit for bit those of stepping
-each member alone.  ``Ensemble.tune`` runs the launch-shape autotuner.
+``Ensemble`` wraps chan_ensemble_* (include/chanrhs.h): a block of L steps
+of every member (L = least common multiple of the members' istat) is
+captured once into a CUDA graph and replayed.  By default that graph holds
+one persistent kernel which runs every member's work units from one work
+list, ordered by per-member device counters with bounded waits
+(``mode="persistent"``); ``mode="graph"`` captures every member's kernels
+instead, one branch per member on its own stream.  Results are bit for bit
+those of stepping each member alone.  ``Ensemble.tune`` runs the
+launch-shape autotuner.
 
 ``sweep_cases`` builds the sweep: cases of uneven grid sizes with per-case
 Mach and Reynolds numbers, a top-bottom wall temperature difference and a
@@ -65,6 +69,23 @@ class Ensemble:
         if r != 0:
             raise ChanError(r, self.L.chan_ensemble_last_error(self._h).decode())
         return ms.value
+
+    MODES = {"graph": _lib.CHAN_ENSEMBLE_GRAPH, "persistent": _lib.CHAN_ENSEMBLE_PERSISTENT,
+             "persistent-stall-test": _lib.CHAN_ENSEMBLE_PERSISTENT_STALL_TEST}
+
+    def set_mode(self, mode: str):
+        """"persistent" (default), "graph", or "persistent-stall-test" (host-side
+        fault injection: a dependency that is never met, for tests)."""
+        r = self.L.chan_ensemble_set_mode(self._h, self.MODES[mode])
+        if r != 0:
+            raise ChanError(r, self.L.chan_ensemble_last_error(self._h).decode())
+
+    def mode_in_use(self):
+        """("persistent" | "graph" | None before the first block, fallback reason)."""
+        m, why = ctypes.c_int32(), ctypes.c_char_p()
+        self.L.chan_ensemble_get_mode(self._h, ctypes.byref(m), ctypes.byref(why))
+        name = {_lib.CHAN_ENSEMBLE_GRAPH: "graph", _lib.CHAN_ENSEMBLE_PERSISTENT: "persistent"}.get(m.value)
+        return name, (why.value or b"").decode()
 
     def counters(self):
         """(graph replays, graph captures) so far."""

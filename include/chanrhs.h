@@ -428,8 +428,9 @@ void chan_free(chan_ctx *c);
  * their own grids, physics, wall BCs and precision -- stepped together.
  * Every member keeps its own buffers and stream.  A block of L steps of all
  * members (L = least common multiple of their istat) is captured once into
- * one CUDA graph, one branch per member, and replayed; the members' kernels
- * run concurrently.  Each member's results are bit for bit those of
+ * one CUDA graph and replayed: by default one persistent kernel that runs
+ * all members' work (chan_ensemble_set_mode below), else one branch of
+ * kernels per member, run concurrently.  Each member's results are bit for bit those of
  * chan_step on that member alone.  A context belongs to one ensemble at most;
  * members may still be used on their own between ensemble calls. */
 typedef struct chan_ensemble chan_ensemble;
@@ -459,6 +460,32 @@ int chan_ensemble_step(chan_ensemble *e, int32_t nsteps, int32_t *status);
  * states, wall rings, statuses and counters are left as they were.  Writes
  * the best trial time (ms per trial step) to best_ms. */
 int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms);
+
+/* How a block of L steps runs (no reference counterpart).
+ * CHAN_ENSEMBLE_PERSISTENT (the default): one persistent kernel per block.
+ *   It walks one work list of every member's units -- the CTAs of each RK
+ *   stage, of each wall-BC pass and of the statistics passes, and the step's
+ *   clock advance -- members interleaved; a unit starts once its member has
+ *   completed its earlier work, which per-member device counters track, and
+ *   each such wait is bounded (about a second).  The block is one graph of
+ *   two nodes (counter reset, the launch).  It needs members of one
+ *   precision, without the closure, on the 32x8 or 16x16 tile; otherwise the
+ *   graph mode is used and chan_ensemble_get_mode says why.
+ * CHAN_ENSEMBLE_GRAPH: one graph of every member's kernels, one branch per
+ *   member on its own stream.
+ * Either way each member's results are bit for bit those of chan_step.
+ * CHAN_ENSEMBLE_PERSISTENT_STALL_TEST: persistent, with member 0's first stage
+ *   made to wait for work that never completes (host-side fault injection
+ *   for tests): chan_ensemble_step then returns CHAN_ECUDA after about a
+ *   second and every member's state is undefined until uploaded again.
+ * chan_ensemble_get_mode reports the mode of the captured block (-1 before
+ * the first capture) and, if persistent mode was asked for but not used, the
+ * reason (an empty string otherwise; valid until the next call). */
+#define CHAN_ENSEMBLE_GRAPH 0
+#define CHAN_ENSEMBLE_PERSISTENT 1
+#define CHAN_ENSEMBLE_PERSISTENT_STALL_TEST 2
+int chan_ensemble_set_mode(chan_ensemble *e, int32_t mode);
+int chan_ensemble_get_mode(chan_ensemble *e, int32_t *in_use, const char **fallback_reason);
 
 /* graph replays and graph captures so far, and the device time (CUDA events
  * on the launching stream) of the graph replays of the last

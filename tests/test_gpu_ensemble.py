@@ -215,3 +215,109 @@ def test_member_blowup_is_reported_for_that_member_only():
     for a, b in zip(good, solo):
         assert np.array_equal(a.download(), b.download())
     e.close()
+
+
+# ---------------------------------------------------------------- persistent mode
+def _members_of(precision):
+    """Two or three contexts of one precision (the persistent kernel runs one
+    precision per ensemble): FP64 with buoyancy and FP64 with a travelling
+    wave; or two mixed-precision sweep cases of uneven grids."""
+    specs = _members()
+    if precision == "fp64":
+        return [specs[0], specs[2]]
+    cs = sweep_cases(3, grids=[(32, 24, 25), (40, 16, 17), (24, 20, 33)], istat=2)
+    return [(f"mixed{i}", (c.params, c.x3, c.jac, c.inv, c.var), lambda g, c=c: g.set_buoyancy(c.Ri or 0.1, 1.0))
+            for i, c in enumerate(cs)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_ensemble_matches_members_alone(precision):
+    """One persistent launch per block: bit for bit the members stepped alone,
+    across replays, remainder steps, statistics steps and time averaging."""
+    specs = _members_of(precision)
+    solo = [_open(s) for s in specs]
+    ens_m = [_open(s) for s in specs]
+    e = Ensemble(ens_m)
+    plan = [13, 5, "avg", 12]
+    for item in plan:
+        if item == "avg":
+            for g in solo + ens_m:
+                g.time_avg_start()
+            continue
+        for g in solo:
+            g.step(item)
+        assert e.step(item) == [0] * len(specs)
+        assert e.mode_in_use() == ("persistent", "")
+    for s, m in zip(solo, ens_m):
+        assert np.array_equal(s.download(), m.download())
+        assert s.nstep == m.nstep and s.time == m.time
+        for a, b in zip(s.stats(), m.stats()):
+            assert np.array_equal(a, b)
+        ta, tb = s.time_average(), m.time_average()
+        assert ta["samples"] == tb["samples"] > 0
+        for k in ("mean", "rms", "covar", "tau"):
+            assert np.array_equal(ta[k], tb[k]), k
+        assert m.debug_canaries() == 0
+    e.close()
+
+
+def test_persistent_mode_falls_back_for_mixed_precisions_and_graph_mode_matches():
+    specs = _members()            # FP64 and mixed members together
+    e = Ensemble([_open(s) for s in specs])
+    e.step(6)
+    assert e.mode_in_use() == ("graph", "members of both precisions")
+    e.close()
+    fp = _members_of("fp64")
+    a = [_open(s) for s in fp]
+    b = [_open(s) for s in fp]
+    ea, eb = Ensemble(a), Ensemble(b)
+    eb.set_mode("graph")
+    ea.step(12)
+    eb.step(12)
+    assert ea.mode_in_use()[0] == "persistent" and eb.mode_in_use()[0] == "graph"
+    for x, y in zip(a, b):
+        assert np.array_equal(x.download(), y.download())
+    ea.close()
+    eb.close()
+
+
+def test_persistent_dependency_wait_gives_up_and_reports():
+    """Host-side fault injection: member 0's first stage waits for work that
+    never completes.  The bounded waits end the launch with CHAN_ECUDA within
+    seconds (no hang), and after a fresh upload the ensemble runs correctly."""
+    import time
+    specs = _members_of("fp64")
+    ens_m = [_open(s) for s in specs]
+    e = Ensemble(ens_m)
+    e.set_mode("persistent-stall-test")
+    t0 = time.time()
+    with pytest.raises(ChanError) as ei:
+        e.step(e.block)
+    assert ei.value.code == _lib.CHAN_ECUDA and "waited more than a second" in str(ei.value)
+    assert time.time() - t0 < 30
+    e.set_mode("persistent")
+    solo = [_open(s) for s in specs]
+    for g, s in zip(ens_m, specs):
+        g.init_sol_v(s[1][4])
+    for g in solo:
+        g.step(6)
+    assert e.step(6) == [0, 0]
+    for x, y in zip(solo, ens_m):
+        assert np.array_equal(x.download(), y.download())
+    e.close()
+
+
+def test_persistent_member_blowup_is_reported_for_that_member_only():
+    specs = _members_of("fp64")
+    good = [_open(specs[0])]
+    solo = [_open(specs[0])]
+    p, x3, jac, inv, var = specs[1][1]
+    bad = Channel(p.with_(dt=p.dt * 400), x3, jac, inv)
+    bad.init_sol_v(var)
+    e = Ensemble(good + [bad])
+    st = e.step(12)
+    assert e.mode_in_use()[0] == "persistent"
+    assert st[0] == 0 and st[1] in (_lib.CHAN_BLOWUP, _lib.CHAN_NONFINITE)
+    solo[0].step(12)
+    assert np.array_equal(good[0].download(), solo[0].download())
+    e.close()
