@@ -300,9 +300,111 @@ def _errors(les, dns):
             "uw_peak": abs(pk(les["uw"]) - pk(dns["uw"])) / pk(dns["uw"])}
 
 
-def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000, snapshots=100, snap_every=200,
-               epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, fp64_probe=400, filter_width=4,
-               log=print):
+def wall_shear_history(ch: Channel, steps: int, every: int):
+    """Step ``steps`` steps in chunks of ``every`` (a multiple of istat) and
+    record (time, wall shear (tauL - tauU)/2) after each chunk."""
+    out = []
+    done = 0
+    while done < steps:
+        n = min(every, steps - done)
+        ch.step(n)
+        done += n
+        tau = ch.stats()[0]
+        out.append((ch.time, 0.5 * (tau[0] - tau[1])))
+    return out
+
+
+def stationarity(hist):
+    """Drift of the wall shear over a window: the least-squares slope times the
+    window length over the mean, and the relative difference of its two halves."""
+    t = np.array([h[0] for h in hist]); w = np.array([h[1] for h in hist])
+    if len(t) < 4:
+        return {"drift": None, "halves": None}
+    slope = np.polyfit(t - t[0], w, 1)[0]
+    h = len(w) // 2
+    return {"tau_w_mean": float(w.mean()), "drift": float(slope * (t[-1] - t[0]) / w.mean()),
+            "halves": float((w[h:].mean() - w[:h].mean()) / w.mean()), "records": len(w)}
+
+
+def scaled_norm(norm, alpha: float):
+    """The closure's normalisation with its outputs scaled by alpha (output
+    means and standard deviations times alpha): the closure's magnitude knob."""
+    n = np.array(norm, dtype=np.float32, copy=True)
+    n[26:44] *= alpha
+    return n
+
+
+def coarse_run(pc: ChanParams, x3, jac, inv, var, steps: int, cl: Closure | None = None, avg_from: float = 0.5,
+               check_every: int = 200):
+    """A coarse run of ``steps`` steps from ``var``, statistics time-averaged over
+    the steps after ``avg_from`` of the run; with ``cl`` the closure is on, with
+    fallback to the plain method."""
+    ch = Channel(pc, x3, jac, inv)
+    ch.init_sol_v(var)
+    first = int(steps * avg_from) // max(pc.istat, 1) * max(pc.istat, 1)
+    t0 = time.time()
+    rep = {"fallback_step": None, "reason": None, "plain_failed": None}
+    try:
+        if cl is None:
+            ch.step(first)
+            ch.time_avg_start()
+            ch.step(steps - first)
+        else:
+            rep = run_with_fallback(ch, cl, first, check_every=check_every)
+            ch.time_avg_start()
+            if rep["fallback_step"] is None:
+                r2 = run_with_fallback(ch, cl, steps - first, check_every=check_every)
+                if r2["fallback_step"] is not None:
+                    rep = r2
+            else:
+                ch.step(steps - first)
+    except BlowUpError as e:
+        rep = {"fallback_step": None, "reason": f"blew up: {e}", "plain_failed": None}
+    wall = time.time() - t0
+    st = None
+    if not (rep["reason"] or "").startswith("blew up") and rep.get("plain_failed") is None:
+        st = _profiles(ch.time_average(), x3, pc.Re)
+    ch.close()
+    return {"steps": steps, "wall_s": wall, "report": rep, "stats": st}
+
+
+def add_shear_deficit(src: Closure, dst: Closure, deficit, per_snapshot: int, per_plane: int, chunk: int = 1 << 22):
+    """Copy the dataset of ``src`` into ``dst`` with the mean Reynolds-shear-
+    stress deficit of the coarse solver added to each sample's tau_uw target:
+    samples come in snapshots of ``per_snapshot`` (per_plane samples per
+    coarse interior plane, planes in order), so sample s sits on coarse plane
+    ((s mod per_snapshot) // per_plane) + 1, whose deficit is added."""
+    n = src.count
+    d = np.asarray(deficit, dtype=np.float64)
+    for first in range(0, n, chunk):
+        m = min(chunk, n - first)
+        X, T = src.data(first, m)
+        idx = np.arange(first, first + m)
+        kc = (idx % per_snapshot) // per_plane + 1
+        T[:, 4] += d[kc].astype(np.float32)
+        dst.add_data(X, T)
+
+
+def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000, snapshots=200, snap_every=200,
+               coarse_steps=20000, epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, cal_seed=21,
+               eval_seed=33, alphas=(0.5, 1.0, 2.0, 3.0), fp64_probe=400, filter_width=4, rec_every=1000, log=print):
+    """The closure experiment.
+
+    1. DNS (mixed precision) from a smooth seeded perturbation, ``spinup``
+       steps, then a window of ``snapshots`` x ``snap_every`` steps in which the
+       width-``filter_width`` filtered DNS is sampled into the dataset and the
+       statistics are time-averaged; the wall shear is recorded every
+       ``rec_every`` steps to show whether the window is stationary.
+    2. A plain coarse run (``coarse_steps`` steps from a seeded smooth
+       perturbation, statistics over its second half) gives what the coarse
+       solver misses: the deficit of its mean Reynolds shear stress rho<u'w'>
+       against the DNS at its wall-normal points.
+    3. Training targets: the filtered-DNS subgrid fluxes, with that deficit
+       added to tau_uw plane by plane.
+    4. The closure's magnitude alpha (its outputs scaled by alpha) is chosen by
+       coarse runs from a calibration seed; the reported comparison, plain
+       against closure, uses coarse runs from another seed.
+    """
     t_all = time.time()
     kst = (dns_grid[2] - 1) // (coarse_grid[2] - 1)
     x3d, jacd, invd = mesh_tanh(dns_grid[2], beta)
@@ -311,26 +413,26 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     pd = pd.with_(dt=cfl_dt(var0, pd, jacd, cfl))
     dns = Channel(pd, x3d, jacd, invd)
     dns.init_sol_v(var0)
-    dns.step(spinup)
-    log(json.dumps({"phase": "dns spin-up", "steps": spinup, "t": dns.time}))
-    # the coarse start: the DNS state at the start of the sampling window
+    rec = rec_every // pd.istat * pd.istat
+    hist_spin = wall_shear_history(dns, spinup, rec)
+    log(json.dumps({"phase": "dns spin-up", "steps": spinup, "t": dns.time,
+                    "last_half": stationarity(hist_spin[len(hist_spin) // 2:])}))
     x3c, jacc, invc = mesh_tanh(coarse_grid[2], beta)
     pc = production_params(coarse_grid)
-    varc = coarsen(dns.download(), pd, pc, kst)
-    pc = pc.with_(dt=cfl_dt(varc, pc, jacc, cfl))
     window = snapshots * snap_every * pd.dt
-    # DNS window: snapshots into the dataset, statistics time-averaged
-    cap = snapshots * ((dns_grid[0] - 3) // 4 + 1) * ((dns_grid[1] - 3) // 3 + 1) * ((dns_grid[2] - 1) // kst - 1)
-    cl = Closure(capacity=cap)
+    per_plane = ((dns_grid[0] - 3) // 4 + 1) * ((dns_grid[1] - 3) // 3 + 1)
+    per_snap = per_plane * ((dns_grid[2] - 1) // kst - 1)
+    raw = Closure(capacity=snapshots * per_snap)
     dns.time_avg_start()
+    hist_win = []
     t0 = time.time()
     for s in range(snapshots):
-        dns.step(snap_every)
-        cl.sample(dns, strides=(4, 3, kst), width=filter_width)
+        hist_win += wall_shear_history(dns, snap_every, snap_every)
+        raw.sample(dns, strides=(4, 3, kst), width=filter_width)
     dns_wall = time.time() - t0
     avg_d = dns.time_average()
     dns_stats = _profiles(avg_d, x3d, pd.Re)
-    # plain FP64 DNS on the same GPU: time a few hundred steps from the window's end state
+    rho_d = np.asarray(avg_d["mean"][0])
     f64 = Channel(pd.with_(mixed=False), x3d, jacd, invd)
     f64.init_sol_v(dns.download())
     f64.step(20)
@@ -338,53 +440,73 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=60000,
     f64.step(fp64_probe)
     fp64_ms = (time.time() - t0) / fp64_probe * 1e3
     f64.close()
-    # the DNS statistics at the coarse grid's wall-normal points
     dns_c = {k: (np.asarray(v)[::kst].tolist() if isinstance(v, list) else v) for k, v in dns_stats.items()}
     dns.close()
-    log(json.dumps({"phase": "dns window", "samples": cl.count, "window_t": window, "wall_s": dns_wall,
-                    "Cf": dns_stats["Cf"], "Re_tau": dns_stats["Re_tau"]}))
-    # training
+    stat = stationarity(hist_win)
+    log(json.dumps({"phase": "dns window", "samples": raw.count, "window_t": window, "wall_s": dns_wall,
+                    "Cf": dns_stats["Cf"], "Re_tau": dns_stats["Re_tau"], "stationarity": stat}))
+
+    # coarse starts and dt: seeded smooth perturbations on the coarse grid
+    def start(sd):
+        v = smooth_start(pc, x3c, seed=sd)
+        return v
+    dtc = cfl_dt(start(cal_seed), pc, jacc, cfl)
+    pcc = pc.with_(dt=dtc)
+    plain_cal = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps)
+    log(json.dumps({"phase": "coarse plain (calibration seed)", "wall_s": plain_cal["wall_s"],
+                    "errors": _errors(plain_cal["stats"], dns_c) if plain_cal["stats"] else None}))
+    # what the coarse solver misses: rho <u'w'> deficit at the coarse points
+    uw_d = np.asarray(dns_c["uw"]) * rho_d[::kst]
+    uw_c = np.asarray(plain_cal["stats"]["uw"]) * rho_d[::kst]
+    deficit = uw_d - uw_c
+    cl = Closure(capacity=raw.count)
+    add_shear_deficit(raw, cl, deficit, per_snap, per_plane)
+    raw.close()
     cl.fit_normalization()
+    norm0 = cl.norm
     cl.init(seed=seed)
     t0 = time.time()
     losses = cl.train(epochs, batch=batch, lr=lr, seed=seed)
     train_s = time.time() - t0
-    log(json.dumps({"phase": "training", "epochs": epochs, "loss_first": float(losses[0]),
+    log(json.dumps({"phase": "training", "epochs": epochs, "samples": cl.count, "loss_first": float(losses[0]),
                     "loss_last": float(losses[-1]), "wall_s": train_s}))
-    # coarse runs over the same window, with and without the closure
-    nc = int(math.ceil(window / pc.dt))
-    runs = {}
-    for name, use in (("closure", True), ("plain", False)):
-        ch = Channel(pc.with_(dt=window / nc), x3c, jacc, invc)
-        ch.init_sol_v(varc)
-        ch.time_avg_start()
-        t0 = time.time()
-        if use:
-            rep = run_with_fallback(ch, cl, nc, check_every=200)
-        else:
-            try:
-                ch.step(nc)
-                rep = {"fallback_step": None, "reason": None}
-            except BlowUpError as e:
-                rep = {"fallback_step": None, "reason": f"plain coarse run blew up: {e}"}
-        wall = time.time() - t0
-        st = _profiles(ch.time_average(), x3c, pc.Re) if rep["reason"] is None or use else None
-        runs[name] = {"steps": nc, "dt": window / nc, "wall_s": wall, "report": rep,
-                      "stats": st, "errors_vs_dns": _errors(st, dns_c) if st else None}
-        ch.close()
-        log(json.dumps({"phase": f"coarse {name}", "steps": nc, "wall_s": wall, "report": rep,
-                        "errors": runs[name]["errors_vs_dns"]}))
+    # a-posteriori calibration of the closure's magnitude (calibration seed)
+    cal = {}
+    for a in alphas:
+        cl.norm = scaled_norm(norm0, a)
+        r = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, cl)
+        e = _errors(r["stats"], dns_c) if r["stats"] and r["report"]["fallback_step"] is None else None
+        cal[a] = {"report": r["report"], "errors": e, "wall_s": r["wall_s"]}
+        log(json.dumps({"phase": "calibration", "alpha": a, **cal[a]}))
+    ok = {a: c for a, c in cal.items() if c["errors"] is not None}
+    best = min(ok, key=lambda a: ok[a]["errors"]["Cf"] + ok[a]["errors"]["uw_peak"]) if ok else None
+    # evaluation from another seed: plain against the calibrated closure
+    runs = {"plain": coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps)}
+    if best is not None:
+        cl.norm = scaled_norm(norm0, best)
+        runs["closure"] = coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps, cl)
+    for name, r in runs.items():
+        r["errors_vs_dns"] = _errors(r["stats"], dns_c) if r["stats"] else None
+        log(json.dumps({"phase": f"coarse {name} (evaluation seed)", "wall_s": r["wall_s"], "report": r["report"],
+                        "errors": r["errors_vs_dns"]}))
     fp64_window_s = fp64_ms * 1e-3 * snapshots * snap_every
-    out = {"dns": {"nP": list(dns_grid), "dt": pd.dt, "window_steps": snapshots * snap_every, "window_t": window,
-                   "wall_s": dns_wall, "stats": dns_c, "precision": "mixed FP32/FP64",
+    fp64_coarse_equiv_s = fp64_ms * 1e-3 * (coarse_steps * pcc.dt / pd.dt)
+    out = {"dns": {"nP": list(dns_grid), "dt": pd.dt, "spinup_steps": spinup, "window_steps": snapshots * snap_every,
+                   "window_t": window, "wall_s": dns_wall, "stats": dns_c, "precision": "mixed FP32/FP64",
+                   "stationarity_window": stat, "stationarity_spinup_last_half": stationarity(
+                       hist_spin[len(hist_spin) // 2:]),
                    "fp64_ms_per_step": fp64_ms, "fp64_window_s": fp64_window_s},
-           "coarse": {"nP": list(coarse_grid), "runs": runs},
+           "coarse": {"nP": list(coarse_grid), "dt": pcc.dt, "steps": coarse_steps, "seeds": {"calibration": cal_seed,
+                                                                                            "evaluation": eval_seed},
+                      "deficit_rho_uw": deficit.tolist(), "calibration": {str(a): c for a, c in cal.items()},
+                      "alpha": best, "runs": runs},
            "training": {"samples": cl.count, "epochs": epochs, "batch": batch, "lr": lr, "filter_width": filter_width,
                         "losses": [float(x) for x in losses], "wall_s": train_s},
-           "wall_time_ratio_dns_over_closure": dns_wall / runs["closure"]["wall_s"],
-           "wall_time_ratio_fp64_dns_over_closure": fp64_window_s / runs["closure"]["wall_s"],
+           "wall_time_fp64_dns_same_physical_time_over_closure":
+               (fp64_coarse_equiv_s / runs["closure"]["wall_s"]) if "closure" in runs else None,
            "total_s": time.time() - t_all}
-    params, norm = cl.params, cl.norm
+    params = cl.params
+    norm = scaled_norm(norm0, best if best is not None else 1.0)
     cl.close()
     return out, params, norm
 
@@ -413,8 +535,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="learned subgrid closure: DNS -> dataset -> training -> coarse runs")
     ap.add_argument("--synthetic-train", type=int, default=0, metavar="N",
                     help="only time training on N synthetic samples (the tensor-core kernel alone)")
-    ap.add_argument("--spinup", type=int, default=60000)
-    ap.add_argument("--snapshots", type=int, default=100)
+    ap.add_argument("--spinup", type=int, default=150000)
+    ap.add_argument("--snapshots", type=int, default=200)
+    ap.add_argument("--coarse-steps", type=int, default=20000)
+    ap.add_argument("--alphas", type=float, nargs="+", default=[0.5, 1.0, 2.0, 3.0])
     ap.add_argument("--snap-every", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--batch", type=int, default=65536)
@@ -430,15 +554,16 @@ def main(argv=None):
         print(json.dumps(synthetic_train(a.synthetic_train, a.epochs, a.batch)), flush=True)
         return 0
     res, params, norm = experiment(tuple(a.dns_grid), tuple(a.coarse_grid), a.spinup, a.snapshots, a.snap_every,
-                                   a.epochs, a.batch, a.lr, filter_width=a.filter_width,
-                                   log=lambda s: print(s, flush=True))
+                                   a.coarse_steps, a.epochs, a.batch, a.lr, alphas=tuple(a.alphas),
+                                   filter_width=a.filter_width, log=lambda s: print(s, flush=True))
     if a.weights:
         np.savez(a.weights, params=params, norm=norm)
     s = json.dumps(res)
     if a.out:
         with open(a.out, "w") as f:
             f.write(s + "\n")
-    print(json.dumps({k: v for k, v in res.items() if k != "coarse"} | {
+    print(json.dumps({k: v for k, v in res.items() if k not in ("coarse", "dns")} | {
+        "alpha": res["coarse"]["alpha"],
         "errors": {n: r["errors_vs_dns"] for n, r in res["coarse"]["runs"].items()},
         "fallback": {n: r["report"] for n, r in res["coarse"]["runs"].items()}}), flush=True)
     return 0

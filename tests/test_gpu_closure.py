@@ -222,3 +222,4 @@ def test_fallback_without_a_workdir_leaves_no_files(monkeypatch, tmp_path):
     rep = run_with_fallback(g, cl, steps=8, check_every=4)
     assert rep["reason"] is not None and g.nstep == 8
     assert list(tmp_path.iterdir()) == []
+

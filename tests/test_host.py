@@ -264,3 +264,47 @@ def test_closure_coarsening_and_smooth_start():
     assert np.allclose(c[6], c[0] * c[5] / (pc.gama * pc.Mac ** 2))
     # periodic duplicates of the coarse field
     assert np.array_equal(c[..., 0], c[..., -2]) and np.array_equal(c[..., -1], c[..., 1])
+
+
+def test_closure_deficit_targets_and_magnitude_knob():
+    """The a-posteriori targets: each sample's tau_uw gets the deficit of the
+    coarse plane it sits on (samples in snapshots, planes in order); the
+    magnitude knob scales only the output half of the normalisation; the
+    stationarity measure sees a drift."""
+    from compchan3dmpi_b200.closure import add_shear_deficit, scaled_norm, stationarity
+
+    class Fake:
+        def __init__(self, X=None, T=None):
+            self.X = [] if X is None else [X]
+            self.T = [] if T is None else [T]
+
+        @property
+        def count(self):
+            return sum(len(x) for x in self.X)
+
+        def data(self, first, n):
+            X, T = np.concatenate(self.X), np.concatenate(self.T)
+            return X[first:first + n].copy(), T[first:first + n].copy()
+
+        def add_data(self, X, T):
+            self.X.append(X)
+            self.T.append(T)
+
+    per_plane, planes, snaps = 5, 3, 2
+    n = per_plane * planes * snaps
+    X = np.arange(n * 13, dtype=np.float32).reshape(n, 13)
+    T = np.zeros((n, 9), np.float32)
+    deficit = np.array([99.0, 1.0, 2.0, 3.0, 99.0])   # coarse planes 0..4; interior 1..3
+    src, dst = Fake(X, T), Fake()
+    add_shear_deficit(src, dst, deficit, per_plane * planes, per_plane, chunk=7)
+    X2, T2 = dst.data(0, n)
+    assert np.array_equal(X2, X)
+    want = np.tile(np.repeat([1.0, 2.0, 3.0], per_plane), snaps)
+    assert np.array_equal(T2[:, 4], want.astype(np.float32))
+    assert np.all(np.delete(T2, 4, axis=1) == 0)
+    norm = np.arange(44, dtype=np.float32)
+    s = scaled_norm(norm, 2.0)
+    assert np.array_equal(s[:26], norm[:26]) and np.array_equal(s[26:], 2 * norm[26:])
+    flat = stationarity([(t, 1.0) for t in range(10)])
+    rising = stationarity([(t, 1.0 + 0.1 * t) for t in range(10)])
+    assert abs(flat["drift"]) < 1e-12 and rising["drift"] > 0.3 and rising["halves"] > 0.2
