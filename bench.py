@@ -205,6 +205,13 @@ def measured_traffic(p, n_int):
         return None, None
 
 
+def upload_bytes(nP):
+    """Bytes chan_upload copies from the host: rho, u, v, w, E everywhere; T
+    and p on the two wall planes and the four corner columns."""
+    n1, n2, n3 = nP
+    return 8 * (5 * n1 * n2 * n3 + 2 * (2 * n1 * n2 + 4 * n3))
+
+
 # --------------------------------------------------------------- CPU
 def cpu_baseline(nP=GRID, budget_s=20.0, threads=None):
     """The oracle (C restatement, OpenMP) on the host cores: one RK3 stage at
@@ -376,7 +383,7 @@ def run_ours(args):
     R.barrier(ranks)
     e2e_ms = R.max_over_ranks(ranks, e0.elapsed_time(e1))
     n_pts = p.nP[0] * p.nP[1] * p.nP[2]
-    h2d = 7 * n_pts * 8
+    h2d = upload_bytes(p.nP)
     d2h = 7 * n_pts * 8 + ncalls * 48 + nstats * (23 * n3 + 2) * 8
 
     status_ok = (st == 0)
@@ -527,7 +534,8 @@ def run_ensemble(args):
                          "kernel": "every member's k_stage (whole ensemble step)",
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
             "e2e": {"value": ranks.world * per_step * K / e2e_max, "unit": UNIT,
-                    "h2d_bytes_per_step": 7 * 8 * n_pts / K, "d2h_bytes_per_step": 7 * 8 * n_pts / K,
+                    "h2d_bytes_per_step": sum(upload_bytes(c.params.nP) for c in cases) / K,
+                    "d2h_bytes_per_step": 7 * 8 * n_pts / K,
                     "calls": "chan_upload of every member + chan_ensemble_step(K) + chan_download of every "
                              "member (host wall clock around the synchronous calls)"},
             "gpu_launches": int(launches),

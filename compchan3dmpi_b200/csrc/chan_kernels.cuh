@@ -1635,9 +1635,14 @@ __global__ void k_upload(const KParams P, const double *var, double *qa, double 
         const int jj = (int)((p / n1) % n2);
         const int kk = (int)(p / ((long long)n1 * n2));
         const int i = ii + 1, j = jj + 1, k = kk + 1;
+        // T and p (columns 5, 6) are read only on the wall planes and the
+        // corner columns: the upload copies them only there
+        const bool wall = (k == 1 || k == n3), corner = (i == 1 || i == n1) && (j == 1 || j == n2);
         double x[7];
 #pragma unroll
-        for (int m = 0; m < 7; m++) x[m] = var[(size_t)m * N + p];
+        for (int m = 0; m < 5; m++) x[m] = var[(size_t)m * N + p];
+        x[5] = (wall || corner) ? var[(size_t)5 * N + p] : 0.0;
+        x[6] = (wall || corner) ? var[(size_t)6 * N + p] : 0.0;
         const long long o = (long long)k * P.plane + (long long)j * P.px + i;
         double q[5] = {x[0], x[0] * x[1], x[0] * x[2], x[0] * x[3], x[0] * x[4]};
 #pragma unroll
@@ -2008,6 +2013,9 @@ __device__ __forceinline__ void pstage(const PPhase &F, const KParams &P, int un
     stage_body<TI, TJ, QI, QO, R, 2, true>(P, F.tm, bx, by, bz, tid % TI, tid / TI, smem);
 }
 
+#ifndef CHAN_PMINB_MIXED
+#define CHAN_PMINB_MIXED 2   // resident CTAs per SM of the mixed-precision persistent kernel (3 spills ~1.3 KB per thread)
+#endif
 template <bool MIXED>
 struct PersistShape {
     // dynamic shared memory: the largest unit's, plus the work-item slot
@@ -2020,7 +2028,7 @@ struct PersistShape {
     static constexpr size_t wall = sizeof(double) * 2 * 6 * kWallHY * kWallHX;
     static constexpr size_t body = ((st > wall ? st : wall) + 127) / 128 * 128;
     static constexpr size_t bytes = body + 128;
-    static constexpr int minb = MIXED ? 3 : 2;
+    static constexpr int minb = MIXED ? CHAN_PMINB_MIXED : 2;
 };
 
 template <bool MIXED>

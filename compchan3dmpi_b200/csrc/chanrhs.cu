@@ -797,8 +797,22 @@ int chan_upload(chan_ctx *c, const double *var, int64_t nstep, double time)
 {
     if (!c || !var) return CHAN_EINVAL;
     CK(c, cudaSetDevice(c->dev));
-    const size_t N = (size_t)c->n1 * c->n2 * c->n3;
-    CK(c, cudaMemcpyAsync(c->dvar, var, 7 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const size_t N = (size_t)c->n1 * c->n2 * c->n3, pl = (size_t)c->n1 * c->n2;
+    // rho, u, v, w, E everywhere; T and p only where they are read: the two
+    // wall planes and the four corner columns (the interior primitives are
+    // derived from the conservative state)
+    CK(c, cudaMemcpyAsync(c->dvar, var, 5 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    for (int m = 5; m < 7; m++) {
+        for (size_t k : {(size_t)0, (size_t)c->n3 - 1})
+            CK(c, cudaMemcpyAsync(c->dvar + m * N + k * pl, var + m * N + k * pl, pl * sizeof(double),
+                                  cudaMemcpyHostToDevice, c->stream));
+        for (size_t jc : {(size_t)0, (size_t)c->n2 - 1})
+            for (size_t ic : {(size_t)0, (size_t)c->n1 - 1}) {
+                const size_t o = m * N + jc * c->n1 + ic;
+                CK(c, cudaMemcpy2DAsync(c->dvar + o, pl * sizeof(double), var + o, pl * sizeof(double),
+                                        sizeof(double), c->n3, cudaMemcpyHostToDevice, c->stream));
+            }
+    }
     chan::k_upload<<<1184, 256, 0, c->stream>>>(c->kp, c->dvar, c->q[0], c->mixed ? c->q[0] : c->q[1],
                                                   c->mixed ? nullptr : c->q[2], c->cs);
     CK(c, cudaGetLastError());
