@@ -69,7 +69,16 @@ def test_mlp_gradients_match_oracle():
     """One training step's loss and gradients (forward, the two data-gradient
     and three weight-gradient products on the tensor cores) against the
     oracle's float64 restatement with the same BF16 roundings; 300 rows, so
-    the last tile is partly empty."""
+    the last tile is partly empty.
+
+    Tolerance: device and oracle round the same quantities to BF16 at the same
+    places.  They differ only where the order of an F32 accumulation (tensor
+    core against numpy, relative differences ~1e-7) moves a value across a
+    BF16 rounding boundary (half an ulp is 2^-9 ~ 2e-3 relative), which
+    changes that element by one BF16 ulp.  Such flips touch a fraction of
+    order 1e-4 of the elements, so a gradient's relative L2 error is ~1e-4
+    (9.6e-5 measured over the whole gradient); the bound per parameter group
+    is 2e-3, 20 times that."""
     cl, params, norm = _random_closure(seed=9)
     rng = np.random.default_rng(2)
     X = rng.standard_normal((300, 13)).astype(np.float32)
@@ -80,7 +89,7 @@ def test_mlp_gradients_match_oracle():
     for name, a, b in (("W1", C.OFF_W1, C.OFF_B1), ("b1", C.OFF_B1, C.OFF_W2), ("W2", C.OFF_W2, C.OFF_B2),
                        ("b2", C.OFF_B2, C.OFF_W3), ("W3", C.OFF_W3, C.OFF_B3), ("b3", C.OFF_B3, C.N_PARAM)):
         e = np.linalg.norm(g[a:b] - go[a:b]) / np.linalg.norm(go[a:b])
-        assert e < 2e-2, (name, e)
+        assert e < 2e-3, (name, e)
 
 
 def test_adam_step_and_training_reduce_the_loss():
