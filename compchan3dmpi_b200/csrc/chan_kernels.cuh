@@ -938,6 +938,16 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
         for (int c = 0; c < 5; c++) q0[c] = sq(iZ, c)[bc];
         if (out_ok) {
+#ifdef CHAN_EARLY_BASE
+            // the RK base of the own point, loaded before the flux sums so that
+            // its latency overlaps them (FP64 rings)
+            double qbe[5] = {0, 0, 0, 0, 0};
+            if (!S::prefetch_base && P.rk_mode != 0) {
+                const long long off = (long long)t * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) qbe[c] = ldq_c<PERSIST>(P.qbase + c * vol + off);
+            }
+#endif
             R Fs[5];   // sum of the flux derivatives
             const R mu0 = smu(mZ)[bc];
             // x
@@ -1040,9 +1050,14 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
                     for (int c = 0; c < 5; c++) qb[c] = sQB[c * NT + tid];
                 } else {
+#ifdef CHAN_EARLY_BASE
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qb[c] = qbe[c];
+#else
                     const long long off = (long long)t * plane + colo;
 #pragma unroll
                     for (int c = 0; c < 5; c++) qb[c] = ldq_c<PERSIST>(P.qbase + c * vol + off);
+#endif
                 }
             }
             if (P.rk_mode == 0) {
