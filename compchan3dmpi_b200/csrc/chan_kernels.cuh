@@ -1989,6 +1989,7 @@ struct PPhase {
     int nx, ny;          // stage: tiles in x, y; wall: blocks in x, y; stats: blocks per plane (S)
     int kp;              // index of the member's KParams record for this phase
     int units;
+    int group;           // wall: wall blocks per unit (the blocks are short)
     unsigned long long need;    // member's completed units before this phase may start
     double dt;                  // clock advance
     const CUtensorMap *tm;      // stage: tensor map of the input buffer
@@ -2105,10 +2106,14 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
             }
             break;
         case kPWall: {
-            const int bx = I.unit % F.nx, r = I.unit / F.nx, by = r % F.ny, wall = r / F.ny;
             WallStage &sp = *reinterpret_cast<WallStage *>(smem_raw);
-            if (F.variant == 0) wall_body<double>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
-            else wall_body<float>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
+            const int nb = F.nx * F.ny * 2, b0 = I.unit * F.group, b1 = min(b0 + F.group, nb);
+            for (int b = b0; b < b1; b++) {
+                if (b > b0) __syncthreads();   // the staging area is reused
+                const int bx = b % F.nx, r = b / F.nx, by = r % F.ny, wall = r / F.ny;
+                if (F.variant == 0) wall_body<double>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
+                else wall_body<float>(P, bx, by, wall, tid % kWallBX, tid / kWallBX, sp);
+            }
             break;
         }
         case kPStatsPart:

@@ -1722,7 +1722,8 @@ int build_persistent(chan_ensemble *e)
                 w.variant = (c->mixed && !last) ? 1 : 0;
                 w.nx = (c->n1 + 2 + chan::kWallBX - 1) / chan::kWallBX;
                 w.ny = (c->n2 + 2 + chan::kWallBY - 1) / chan::kWallBY;
-                w.units = w.nx * w.ny * 2;
+                w.group = 8;
+                w.units = (w.nx * w.ny * 2 + w.group - 1) / w.group;
                 w.kp = kp0 + it - 1;
                 add(w);
             }
