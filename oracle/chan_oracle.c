@@ -82,6 +82,8 @@ typedef struct {
     double *wuv[2], *wx1[2];
     /* buoyancy body force (orc_set_buoyancy); ri = 0: off */
     double ri, tref;
+    /* 1: the v1.9 binary's single-rank reads of var beyond its bounds (orc_set_v19_alias) */
+    int v19alias;
 } orc_t;
 
 #define ID(o, i, j, k) ((((size_t)(k)) * (o)->NJ + (size_t)(j)) * (o)->NI + (size_t)(i))
@@ -93,6 +95,27 @@ typedef struct {
 #define GD(o, m, i, j, k) (o)->gD[(size_t)((m) - 1) * (o)->NP + ID(o, i, j, k)]
 #define HD(o, m, i, j, k) (o)->hD[(size_t)((m) - 1) * (o)->NP + ID(o, i, j, k)]
 #define FF(o, a, m, i, j, k) (o)->a[(size_t)((m) - 1) * (o)->NP + ID(o, i, j, k)]
+
+/* var(i,j,k,m) as the 4th-order central fluxes read it.  main19fix
+ * (v1.10/codes/main_v1.9.f90:44) declares var(0:nP+1,...) and fills the
+ * periodic ghosts; v1.9 (v1.9/codes/main_v1.9.f90:38) declares
+ * var(nP1,nP2,nP3,7) without ghosts, yet the central branch reads var(i+-2,...)
+ * and var(...,j+-2,...) (main_v1.9.f90:348-351, 386-389).  On one rank those
+ * reads land, through the column-major layout, on the neighbouring column or
+ * plane of the same variable: var(nP1+1,j,k) is var(1,j+1,k), var(0,j,k) is
+ * var(nP1,j-1,k), var(i,nP2+1,k) is var(i,1,k+1) and var(i,0,k) is
+ * var(i,nP2,k-1).  For interior points (2 <= i <= nP1-1, 2 <= j <= nP2-1,
+ * 2 <= k <= nP3-1) every such read stays inside the array. */
+static inline double var_c(const orc_t *o, int m, int i, int j, int k)
+{
+    if (o->v19alias) {
+        if (i == o->n1 + 1) { i = 1; j++; }
+        else if (i == 0) { i = o->n1; j--; }
+        if (j == o->n2 + 1) { j = 1; k++; }
+        else if (j == 0) { j = o->n2; k--; }
+    }
+    return VAR(o, m, i, j, k);
+}
 
 static const double haf = 0.5, two = 2.0, zer = 0.0, one = 1.0;
 static const double two3rd = 2.0 / 3.0, one12th = 1.0 / 12.0;
@@ -309,6 +332,10 @@ void orc_upload(orc_t *o, const double *v, long nstep, double time)
 }
 
 /* Forcing state (the lagged wall shear and plane-mean density) */
+/* on = 1: the canonical v1.9 binary's aliased var reads (var_c above);
+ * on = 0 (default): main19fix's true periodic ghosts */
+void orc_set_v19_alias(orc_t *o, int on) { o->v19alias = on ? 1 : 0; }
+
 void orc_set_buoyancy(orc_t *o, double ri, double tref)
 {
     o->ri = ri;
@@ -383,10 +410,10 @@ void orc_stage(orc_t *o, int iter)
                 } else {
                     for (m = 1; m <= 5; m++)
                         FF(o, F1, m, i, j, k) =
-                            (-(VAR(o, 2, i + 2, j, k) * SOLV(o, 0, m, i + 2, j, k))
+                            (-(var_c(o, 2, i + 2, j, k) * SOLV(o, 0, m, i + 2, j, k))
                              + 8.0 * VAR(o, 2, i + 1, j, k) * SOLV(o, 0, m, i + 1, j, k)
                              - 8.0 * VAR(o, 2, i - 1, j, k) * SOLV(o, 0, m, i - 1, j, k)
-                             + VAR(o, 2, i - 2, j, k) * SOLV(o, 0, m, i - 2, j, k)) * invdx * one12th;
+                             + var_c(o, 2, i - 2, j, k) * SOLV(o, 0, m, i - 2, j, k)) * invdx * one12th;
                 }
                 Pe = Re * fabs(SOLV(o, 0, 3, i, j, k)) * dy / MU(o, i, j, k);
                 if (Pe > o->PeyVal) {
@@ -399,10 +426,10 @@ void orc_stage(orc_t *o, int iter)
                 } else {
                     for (m = 1; m <= 5; m++)
                         FF(o, G1, m, i, j, k) =
-                            (-(VAR(o, 3, i, j + 2, k) * SOLV(o, 0, m, i, j + 2, k))
+                            (-(var_c(o, 3, i, j + 2, k) * SOLV(o, 0, m, i, j + 2, k))
                              + 8.0 * VAR(o, 3, i, j + 1, k) * SOLV(o, 0, m, i, j + 1, k)
                              - 8.0 * VAR(o, 3, i, j - 1, k) * SOLV(o, 0, m, i, j - 1, k)
-                             + VAR(o, 3, i, j - 2, k) * SOLV(o, 0, m, i, j - 2, k)) * invdy * one12th;
+                             + var_c(o, 3, i, j - 2, k) * SOLV(o, 0, m, i, j - 2, k)) * invdy * one12th;
                 }
                 Pe = Re * fabs(SOLV(o, 0, 4, i, j, k)) * dXi * o->jac[k] / MU(o, i, j, k);
                 if (k < 3 || k > n3 - 2) {

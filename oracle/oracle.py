@@ -68,6 +68,7 @@ def lib():
         L.orc_get_stats.argtypes = [ctypes.c_void_p, _D, _D, _D, _D]
         L.orc_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D]
         L.orc_set_buoyancy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        L.orc_set_v19_alias.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_wall_bc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, _D, ctypes.c_void_p, _D, _D]
         L.orc_diagnostics.argtypes = [_D, _I, _I, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, _D]
@@ -185,6 +186,13 @@ class Oracle:
     def set_forcing(self, tauL, tauU, rhobar):
         rb = np.ascontiguousarray(rhobar, dtype=np.float64)
         lib().orc_set_forcing(self._h, float(tauL), float(tauU), _dp(rb))
+
+    def set_v19_alias(self, on=True):
+        """The canonical v1.9 binary's single-rank semantics: its 4th-order
+        central fluxes read var(i+-2) / var(j+-2) beyond var's bounds, which land
+        on the neighbouring column or plane (chan_oracle.c, var_c).  Off by
+        default: main19fix's periodic ghosts."""
+        lib().orc_set_v19_alias(self._h, 1 if on else 0)
 
     def set_buoyancy(self, Ri, Tref=1.0):
         """Same buoyancy body force as Channel.set_buoyancy."""

@@ -182,3 +182,40 @@ def test_closure_oracle_gradient_matches_finite_differences():
             assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(g[idx])), (idx, fd, g[idx])
     finally:
         C.bf16 = orig
+
+
+def test_v19_alias_changes_only_the_edge_points_of_one_stage():
+    """The v1.9 aliasing switch: with the central branch everywhere, one stage
+    differs from main19fix's only at the points whose x or spanwise 4th-order
+    stencil reaches past the ghost-free var (i = 2, nP1-1 or j = 2, nP2-1) and
+    their periodic duplicates; everywhere else the two agree bit for bit.  At such a point the
+    difference is the one the aliased reads imply: var(0,j,k) is var(nP1,j-1,k)
+    instead of var(nP1-2,j,k)."""
+    from chan_cases import make_case
+    p, x3, jac, inv, var = make_case(nP=(12, 10, 9), Pe=(1e300, 1e300, 1e300), quantize=False)
+    a = O.Oracle(p, x3, jac, inv)
+    b = O.Oracle(p, x3, jac, inv)
+    b.set_v19_alias(True)
+    for o in (a, b):
+        o.upload(var)
+        o.stage(1)
+    qa, qb = a.download_solv(0), b.download_solv(0)
+    n1, n2, n3 = p.nP
+    d = np.any(qa != qb, axis=0)            # [k][j][i], 0-based
+    edge = np.zeros_like(d)                 # the edge points and their periodic duplicates
+    for i in (0, 1, n1 - 2, n1 - 1):
+        edge[1:n3 - 1, :, i] = True
+    for j in (0, 1, n2 - 2, n2 - 1):
+        edge[1:n3 - 1, j, :] = True
+    assert not np.any(d & ~edge)
+    assert np.all(d[1:n3 - 1, 2:n2 - 2, 1])     # every interior-row point at i = 2 changes
+    # the x-flux difference at (i=2, j, k) from the two wraps of var(0, j, k)
+    k, j = 3, 4                                 # 1-based interior point (2, j, k)
+    u = var[1]                                  # [k][j][i] 0-based
+    rho = var[0]
+    diff_u0 = u[k - 1, j - 2, n1 - 1] - u[k - 1, j - 1, n1 - 3]   # var(nP1,j-1,k) - var(nP1-2,j,k)
+    Q0 = rho[k - 1, j - 1, n1 - 3]              # solV(0,j,k,1) = its periodic image (nP1-2,j,k)
+    dF = diff_u0 * Q0 * (1.0 / p.dx) / 12.0     # F(:,1) gains +var(i-2)*solV(i-2)/(12 dx)
+    cdt = 0.5 * p.dt                            # RK2 stage 1: Q <- Q + dt/2 * R, R = -dF
+    got = qb[0, k - 1, j - 1, 1] - qa[0, k - 1, j - 1, 1]
+    assert abs(got - (-cdt * dF)) <= 1e-12 * abs(cdt * dF) + 1e-15, (got, -cdt * dF)
