@@ -480,6 +480,13 @@ def run_ensemble(args):
     e.step(W)
     st1 = e.step(K)
     tuned_ms = e.last_replay_ms()
+    mode, fallback = e.mode_in_use()
+    # the same tuned shapes in the other mode: every member's kernels in one graph
+    e.set_mode("graph")
+    e.step(W)
+    stg = e.step(K)
+    graph_ms = e.last_replay_ms()
+    e.set_mode("persistent")
     ck = clocks.stop()
     shapes = e.launch_shapes()
     replays, captures = e.counters()
@@ -527,6 +534,9 @@ def run_ensemble(args):
             "one_at_a_time": {"value": solo, "ms_per_step": solo_max / K,
                               "how": "each case alone, default launch shape, CUDA events on its stream"},
             "speedup_vs_one_at_a_time": value / solo,
+            "mode": mode, "mode_fallback_reason": fallback,
+            "graph_mode": {"value": per_step * K / (graph_ms / 1e3), "ms_per_step": graph_ms / K,
+                           "how": "same members and shapes, every member's kernels replayed from one graph"},
             "untuned": {"value": per_step * K / (untuned_ms / 1e3), "ms_per_step": untuned_ms / K},
             "autotuner": {"trial_ms": tune_ms, "shapes": [list(x) for x in shapes]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -540,7 +550,7 @@ def run_ensemble(args):
                              "member (host wall clock around the synchronous calls)"},
             "gpu_launches": int(launches),
             "graph": {"replays": replays, "captures": captures},
-            "status_ok": all(x == 0 for x in st0 + st1 + st2),
+            "status_ok": all(x == 0 for x in st0 + st1 + st2 + stg),
         }
         if ck:
             line["clocks"] = ck
