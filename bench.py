@@ -17,8 +17,9 @@ double accumulation) on the same workload and adds its error against the
 FP64 path.
 
 --ensemble measures the stratified parameter sweep (16 mixed-precision cases
-of uneven grids) stepped as one graph-replayed ensemble with autotuned launch
-shapes, next to the same cases run one at a time.
+of uneven grids) stepped as one ensemble with autotuned launch shapes -- one
+persistent kernel per block of steps, and for comparison every member's
+kernels replayed from one graph -- next to the same cases run one at a time.
 """
 from __future__ import annotations
 
