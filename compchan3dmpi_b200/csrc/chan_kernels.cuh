@@ -580,7 +580,11 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     using Slot = SlotT<R>;
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT, MPW = S::MPW, QSLOT = S::QSLOT;
     // boxes by bulk tensor copy when the input is stored in the ring type
+#ifdef CHAN_NO_TMA
+    constexpr bool TMA = false;   // measurement variant: per-thread box loads into the same ring
+#else
     constexpr bool TMA = std::is_same<QI, R>::value;
+#endif
     static_assert(2 * TJ <= 32 && 32 + 2 * TI <= NT, "halo-flux lane layout needs 2*TJ <= 32 and 32+2*TI <= TI*TJ");
     R *sQ = reinterpret_cast<R *>(smem_raw);                       // [3 slots][5][NB]
     R *sPr = reinterpret_cast<R *>(smem_raw + S::q_bytes);         // [2][4][NB] u,v,w,T
