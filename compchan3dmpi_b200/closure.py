@@ -335,10 +335,13 @@ def scaled_norm(norm, alpha: float):
 
 
 def coarse_run(pc: ChanParams, x3, jac, inv, var, steps: int, cl: Closure | None = None, avg_from: float = 0.5,
-               check_every: int = 200):
+               check_every: int = 200, sample_into: Closure | None = None, sample_every: int = 200):
     """A coarse run of ``steps`` steps from ``var``, statistics time-averaged over
     the steps after ``avg_from`` of the run; with ``cl`` the closure is on, with
-    fallback to the plain method."""
+    fallback to the plain method.  With ``sample_into`` (plain runs) the run's
+    own closure inputs -- every interior point, no filter, the features the
+    closure would see -- are sampled every ``sample_every`` steps of the
+    averaging window."""
     ch = Channel(pc, x3, jac, inv)
     ch.init_sol_v(var)
     first = int(steps * avg_from) // max(pc.istat, 1) * max(pc.istat, 1)
@@ -348,7 +351,15 @@ def coarse_run(pc: ChanParams, x3, jac, inv, var, steps: int, cl: Closure | None
         if cl is None:
             ch.step(first)
             ch.time_avg_start()
-            ch.step(steps - first)
+            if sample_into is None:
+                ch.step(steps - first)
+            else:
+                done = first
+                while done < steps:
+                    n = min(sample_every, steps - done)
+                    ch.step(n)
+                    done += n
+                    sample_into.sample(ch, strides=(1, 1, 1), width=0)
         else:
             rep = run_with_fallback(ch, cl, first, check_every=check_every)
             ch.time_avg_start()
@@ -385,9 +396,42 @@ def add_shear_deficit(src: Closure, dst: Closure, deficit, per_snapshot: int, pe
         dst.add_data(X, T)
 
 
+def _train_and_calibrate(name, sources, deficit, pcc, x3c, jacc, invc, start, cal_seed, coarse_steps, dns_c, epochs,
+                         batch, lr, seed, alphas, log):
+    """One training set: the samples of ``sources`` (closure datasets with their
+    snapshot layout) with the coarse solver's shear-stress deficit added to
+    tau_uw; training; the magnitude alpha picked by coarse runs from the
+    calibration seed.  Returns (closure, normalisation, alpha, report)."""
+    cl = Closure(capacity=sum(src.count for src, _, _ in sources))
+    for src, per_snap, per_plane in sources:
+        add_shear_deficit(src, cl, deficit, per_snap, per_plane)
+    cl.fit_normalization()
+    norm0 = cl.norm
+    cl.init(seed=seed)
+    t0 = time.time()
+    losses = cl.train(epochs, batch=batch, lr=lr, seed=seed)
+    train_s = time.time() - t0
+    log(json.dumps({"phase": f"training ({name})", "epochs": epochs, "samples": cl.count,
+                    "loss_first": float(losses[0]), "loss_last": float(losses[-1]), "wall_s": train_s}))
+    cal = {}
+    for a in alphas:
+        cl.norm = scaled_norm(norm0, a)
+        r = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, cl)
+        e = _errors(r["stats"], dns_c) if r["stats"] and r["report"]["fallback_step"] is None else None
+        cal[a] = {"report": r["report"], "errors": e, "wall_s": r["wall_s"]}
+        log(json.dumps({"phase": f"calibration ({name})", "alpha": a, **cal[a]}))
+    ok = {a: c for a, c in cal.items() if c["errors"] is not None}
+    best = min(ok, key=lambda a: ok[a]["errors"]["Cf"] + ok[a]["errors"]["uw_peak"]) if ok else None
+    rep = {"samples": cl.count, "losses": [float(x) for x in losses], "train_s": train_s,
+           "calibration": {str(a): c for a, c in cal.items()}, "alpha": best,
+           "score": (ok[best]["errors"]["Cf"] + ok[best]["errors"]["uw_peak"]) if best is not None else None}
+    return cl, norm0, best, rep
+
+
 def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000, snapshots=200, snap_every=200,
                coarse_steps=20000, epochs=20, batch=65536, lr=1e-3, cfl=0.6, beta=2.2, seed=7, cal_seed=21,
-               eval_seed=33, alphas=(0.5, 1.0, 2.0, 3.0), fp64_probe=400, filter_width=4, rec_every=1000, log=print):
+               eval_seed=33, alphas=(0.5, 1.0, 2.0, 3.0), fp64_probe=400, filter_width=4, rec_every=1000,
+               coarse_snapshots=50, Re=None, log=print):
     """The closure experiment.
 
     1. DNS (mixed precision) from a smooth seeded perturbation, ``spinup``
@@ -398,27 +442,35 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
     2. A plain coarse run (``coarse_steps`` steps from a seeded smooth
        perturbation, statistics over its second half) gives what the coarse
        solver misses: the deficit of its mean Reynolds shear stress rho<u'w'>
-       against the DNS at its wall-normal points.
-    3. Training targets: the filtered-DNS subgrid fluxes, with that deficit
-       added to tau_uw plane by plane.
-    4. The closure's magnitude alpha (its outputs scaled by alpha) is chosen by
-       coarse runs from a calibration seed; the reported comparison, plain
-       against closure, uses coarse runs from another seed.
+       against the DNS at its wall-normal points.  ``coarse_snapshots`` of its
+       own closure inputs are sampled over the same half.
+    3. Two training sets, each with that deficit added to tau_uw plane by
+       plane: the filtered-DNS samples with their subgrid fluxes, and those plus
+       the coarse run's own inputs (deficit targets only), which are the inputs
+       the closure meets in a coarse run.
+    4. For each, the closure's magnitude alpha (its outputs scaled by alpha) is
+       chosen by coarse runs from a calibration seed; the better training set
+       by that score is then compared, plain against closure, in coarse runs
+       from another seed.
     """
     t_all = time.time()
     kst = (dns_grid[2] - 1) // (coarse_grid[2] - 1)
     x3d, jacd, invd = mesh_tanh(dns_grid[2], beta)
     pd = production_params(dns_grid).with_(mixed=True)
+    if Re is not None:
+        pd = pd.with_(Re=Re)
     var0 = smooth_start(pd, x3d, seed=seed)
     pd = pd.with_(dt=cfl_dt(var0, pd, jacd, cfl))
     dns = Channel(pd, x3d, jacd, invd)
     dns.init_sol_v(var0)
-    rec = rec_every // pd.istat * pd.istat
+    rec = max(rec_every // pd.istat, 1) * pd.istat
     hist_spin = wall_shear_history(dns, spinup, rec)
     log(json.dumps({"phase": "dns spin-up", "steps": spinup, "t": dns.time,
                     "last_half": stationarity(hist_spin[len(hist_spin) // 2:])}))
     x3c, jacc, invc = mesh_tanh(coarse_grid[2], beta)
     pc = production_params(coarse_grid)
+    if Re is not None:
+        pc = pc.with_(Re=Re)
     window = snapshots * snap_every * pd.dt
     per_plane = ((dns_grid[0] - 3) // 4 + 1) * ((dns_grid[1] - 3) // 3 + 1)
     per_snap = per_plane * ((dns_grid[2] - 1) // kst - 1)
@@ -448,41 +500,34 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
 
     # coarse starts and dt: seeded smooth perturbations on the coarse grid
     def start(sd):
-        v = smooth_start(pc, x3c, seed=sd)
-        return v
+        return smooth_start(pc, x3c, seed=sd)
     dtc = cfl_dt(start(cal_seed), pc, jacc, cfl)
     pcc = pc.with_(dt=dtc)
-    plain_cal = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps)
+    c1, c2, c3 = coarse_grid
+    cper_plane, cper_snap = (c1 - 2) * (c2 - 2), (c1 - 2) * (c2 - 2) * (c3 - 2)
+    craw = Closure(capacity=(coarse_snapshots + 1) * cper_snap)
+    every = max(((coarse_steps - coarse_steps // 2) // max(coarse_snapshots, 1)) // pcc.istat, 1) * pcc.istat
+    plain_cal = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, sample_into=craw,
+                           sample_every=every)
     log(json.dumps({"phase": "coarse plain (calibration seed)", "wall_s": plain_cal["wall_s"],
+                    "samples": craw.count,
                     "errors": _errors(plain_cal["stats"], dns_c) if plain_cal["stats"] else None}))
     # what the coarse solver misses: rho <u'w'> deficit at the coarse points
     uw_d = np.asarray(dns_c["uw"]) * rho_d[::kst]
     uw_c = np.asarray(plain_cal["stats"]["uw"]) * rho_d[::kst]
     deficit = uw_d - uw_c
-    cl = Closure(capacity=raw.count)
-    add_shear_deficit(raw, cl, deficit, per_snap, per_plane)
-    raw.close()
-    cl.fit_normalization()
-    norm0 = cl.norm
-    cl.init(seed=seed)
-    t0 = time.time()
-    losses = cl.train(epochs, batch=batch, lr=lr, seed=seed)
-    train_s = time.time() - t0
-    log(json.dumps({"phase": "training", "epochs": epochs, "samples": cl.count, "loss_first": float(losses[0]),
-                    "loss_last": float(losses[-1]), "wall_s": train_s}))
-    # a-posteriori calibration of the closure's magnitude (calibration seed)
-    cal = {}
-    for a in alphas:
-        cl.norm = scaled_norm(norm0, a)
-        r = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, cl)
-        e = _errors(r["stats"], dns_c) if r["stats"] and r["report"]["fallback_step"] is None else None
-        cal[a] = {"report": r["report"], "errors": e, "wall_s": r["wall_s"]}
-        log(json.dumps({"phase": "calibration", "alpha": a, **cal[a]}))
-    ok = {a: c for a, c in cal.items() if c["errors"] is not None}
-    best = min(ok, key=lambda a: ok[a]["errors"]["Cf"] + ok[a]["errors"]["uw_peak"]) if ok else None
+    sets = {"filtered DNS": [(raw, per_snap, per_plane)],
+            "filtered DNS + coarse inputs": [(raw, per_snap, per_plane), (craw, cper_snap, cper_plane)]}
+    trained = {}
+    for name, srcs in sets.items():
+        trained[name] = _train_and_calibrate(name, srcs, deficit, pcc, x3c, jacc, invc, start, cal_seed,
+                                             coarse_steps, dns_c, epochs, batch, lr, seed, alphas, log)
+    ok = {n: t for n, t in trained.items() if t[2] is not None}
+    chosen = min(ok, key=lambda n: ok[n][3]["score"]) if ok else None
     # evaluation from another seed: plain against the calibrated closure
     runs = {"plain": coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps)}
-    if best is not None:
+    if chosen is not None:
+        cl, norm0, best, _ = trained[chosen]
         cl.norm = scaled_norm(norm0, best)
         runs["closure"] = coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps, cl)
     for name, r in runs.items():
@@ -491,23 +536,27 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
                         "errors": r["errors_vs_dns"]}))
     fp64_window_s = fp64_ms * 1e-3 * snapshots * snap_every
     fp64_coarse_equiv_s = fp64_ms * 1e-3 * (coarse_steps * pcc.dt / pd.dt)
-    out = {"dns": {"nP": list(dns_grid), "dt": pd.dt, "spinup_steps": spinup, "window_steps": snapshots * snap_every,
-                   "window_t": window, "wall_s": dns_wall, "stats": dns_c, "precision": "mixed FP32/FP64",
-                   "stationarity_window": stat, "stationarity_spinup_last_half": stationarity(
-                       hist_spin[len(hist_spin) // 2:]),
+    out = {"dns": {"nP": list(dns_grid), "Re": pd.Re, "dt": pd.dt, "spinup_steps": spinup,
+                   "window_steps": snapshots * snap_every, "window_t": window, "wall_s": dns_wall, "stats": dns_c,
+                   "precision": "mixed FP32/FP64", "stationarity_window": stat,
+                   "stationarity_spinup_last_half": stationarity(hist_spin[len(hist_spin) // 2:]),
                    "fp64_ms_per_step": fp64_ms, "fp64_window_s": fp64_window_s},
-           "coarse": {"nP": list(coarse_grid), "dt": pcc.dt, "steps": coarse_steps, "seeds": {"calibration": cal_seed,
-                                                                                            "evaluation": eval_seed},
-                      "deficit_rho_uw": deficit.tolist(), "calibration": {str(a): c for a, c in cal.items()},
-                      "alpha": best, "runs": runs},
-           "training": {"samples": cl.count, "epochs": epochs, "batch": batch, "lr": lr, "filter_width": filter_width,
-                        "losses": [float(x) for x in losses], "wall_s": train_s},
+           "coarse": {"nP": list(coarse_grid), "dt": pcc.dt, "steps": coarse_steps,
+                      "seeds": {"calibration": cal_seed, "evaluation": eval_seed},
+                      "deficit_rho_uw": deficit.tolist(), "training_sets": {n: t[3] for n, t in trained.items()},
+                      "chosen": chosen, "alpha": trained[chosen][2] if chosen else None, "runs": runs},
            "wall_time_fp64_dns_same_physical_time_over_closure":
                (fp64_coarse_equiv_s / runs["closure"]["wall_s"]) if "closure" in runs else None,
            "total_s": time.time() - t_all}
-    params = cl.params
-    norm = scaled_norm(norm0, best if best is not None else 1.0)
-    cl.close()
+    if chosen is not None:
+        cl, norm0, best, _ = trained[chosen]
+        params, norm = cl.params, scaled_norm(norm0, best)
+    else:
+        params, norm = None, None
+    for t in trained.values():
+        t[0].close()
+    raw.close()
+    craw.close()
     return out, params, norm
 
 
@@ -547,6 +596,10 @@ def main(argv=None):
     ap.add_argument("--coarse-grid", type=int, nargs=3, default=[64, 64, 65])
     ap.add_argument("--filter-width", type=int, default=4,
                     help="box-filter width (even, in DNS points) in x and spanwise for the training targets")
+    ap.add_argument("--cfl", type=float, default=0.6)
+    ap.add_argument("--re", type=float, default=None, help="Reynolds number (default: the production 3000)")
+    ap.add_argument("--coarse-snapshots", type=int, default=50)
+    ap.add_argument("--rec-every", type=int, default=1000)
     ap.add_argument("--out", default=None, help="write the JSON report here")
     ap.add_argument("--weights", default=None, help="save the trained closure (npz) here")
     a = ap.parse_args(argv)
@@ -554,16 +607,17 @@ def main(argv=None):
         print(json.dumps(synthetic_train(a.synthetic_train, a.epochs, a.batch)), flush=True)
         return 0
     res, params, norm = experiment(tuple(a.dns_grid), tuple(a.coarse_grid), a.spinup, a.snapshots, a.snap_every,
-                                   a.coarse_steps, a.epochs, a.batch, a.lr, alphas=tuple(a.alphas),
-                                   filter_width=a.filter_width, log=lambda s: print(s, flush=True))
-    if a.weights:
+                                   a.coarse_steps, a.epochs, a.batch, a.lr, cfl=a.cfl, alphas=tuple(a.alphas),
+                                   filter_width=a.filter_width, rec_every=a.rec_every,
+                                   coarse_snapshots=a.coarse_snapshots, Re=a.re, log=lambda s: print(s, flush=True))
+    if a.weights and params is not None:
         np.savez(a.weights, params=params, norm=norm)
     s = json.dumps(res)
     if a.out:
         with open(a.out, "w") as f:
             f.write(s + "\n")
     print(json.dumps({k: v for k, v in res.items() if k not in ("coarse", "dns")} | {
-        "alpha": res["coarse"]["alpha"],
+        "alpha": res["coarse"]["alpha"], "chosen": res["coarse"]["chosen"],
         "errors": {n: r["errors_vs_dns"] for n, r in res["coarse"]["runs"].items()},
         "fallback": {n: r["report"] for n, r in res["coarse"]["runs"].items()}}), flush=True)
     return 0
