@@ -145,7 +145,8 @@ SIGNATURES = [
 CHAN_TILE_32x8 = 0
 CHAN_TILE_32x4 = 1
 CHAN_TILE_16x16 = 2
-CHAN_NTILES = 3
+CHAN_TILE_32x16 = 3
+CHAN_NTILES = 4
 CHAN_ENSEMBLE_GRAPH = 0
 CHAN_ENSEMBLE_PERSISTENT = 1
 CHAN_ENSEMBLE_PERSISTENT_STALL_TEST = 2

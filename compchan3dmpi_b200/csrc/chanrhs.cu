@@ -47,9 +47,9 @@ StageSet make_stage_set()
     s.smemf = chan::StageShape<TI_, TJ_, float>::bytes;
     return s;
 }
-// CHAN_TILE_32x8 (default), CHAN_TILE_32x4, CHAN_TILE_16x16
+// CHAN_TILE_32x8 (default), CHAN_TILE_32x4, CHAN_TILE_16x16, CHAN_TILE_32x16
 const StageSet kStageSets[CHAN_NTILES] = {make_stage_set<32, 8>(), make_stage_set<32, 4>(),
-                                          make_stage_set<16, 16>()};
+                                          make_stage_set<16, 16>(), make_stage_set<32, 16>()};
 constexpr int kMaxSplit = 16;   // statistics blocks per plane, at most
 
 std::string g_init_error;
@@ -1670,7 +1670,7 @@ std::string persistent_blocker(const chan_ensemble *e)
     for (chan_ctx *c : e->m) {
         if (c->mixed != mixed) return "members of both precisions";
         if (c->closure_on) return "a member runs with the learned closure";
-        if (c->tile != CHAN_TILE_32x8 && c->tile != CHAN_TILE_16x16) return "a member uses the 32x4 tile";
+        if (c->tile != CHAN_TILE_32x8 && c->tile != CHAN_TILE_16x16) return "a member uses a tile of other than 256 threads";
     }
     return "";
 }
@@ -2033,7 +2033,7 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
         const int nz = c->n3 - 2;
         const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
         for (int t = 0; t < CHAN_NTILES; t++) {
-            if (e->mode == CHAN_ENSEMBLE_PERSISTENT && t == CHAN_TILE_32x4) continue;   // 128-thread CTAs
+            if (e->mode == CHAN_ENSEMBLE_PERSISTENT && (t == CHAN_TILE_32x4 || t == CHAN_TILE_32x16)) continue;
             int last = -1;
             for (int d : depth) {
                 const int nc = std::max(1, (nz + std::min(d, nz) - 1) / std::min(d, nz));
@@ -2059,7 +2059,8 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms)
         const int depth[] = {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 100000};
         for (int t = 0; t < CHAN_NTILES && rc == CHAN_OK; t++)
             for (int d : depth) {
-                if (e->mode == CHAN_ENSEMBLE_PERSISTENT && t == CHAN_TILE_32x4) continue;   // 128-thread CTAs
+                if (e->mode == CHAN_ENSEMBLE_PERSISTENT && (t == CHAN_TILE_32x4 || t == CHAN_TILE_32x16))
+                    continue;   // the persistent kernel runs 256-thread CTAs
                 std::vector<int> tt(n, t), cc(n);
                 for (size_t i = 0; i < n; i++) {
                     const int nz = e->m[i]->n3 - 2, dd = std::min(d, nz);

@@ -220,7 +220,8 @@ int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc);
 
 /* Stage-kernel launch shape (no reference counterpart; it changes no result
  * bits).  tile: CHAN_TILE_32x8 (256 threads, the default), CHAN_TILE_32x4
- * (128 threads) or CHAN_TILE_16x16 (256 threads) columns x rows per CTA;
+ * (128 threads), CHAN_TILE_16x16 (256 threads) or CHAN_TILE_32x16 (512
+ * threads, one CTA per SM) columns x rows per CTA;
  * nchunks: how many CTAs split the
  * wall-normal march of one tile column (1..nP3-2; 0 picks the count that fills
  * whole waves of resident CTAs, as chan_init does).  chan_get_launch reports
@@ -228,7 +229,8 @@ int chan_set_wall_bc(chan_ctx *c, int32_t wall, const chan_wall_bc *bc);
 #define CHAN_TILE_32x8 0
 #define CHAN_TILE_32x4 1
 #define CHAN_TILE_16x16 2
-#define CHAN_NTILES 3
+#define CHAN_TILE_32x16 3
+#define CHAN_NTILES 4
 int chan_set_launch(chan_ctx *c, int32_t tile, int32_t nchunks);
 int chan_get_launch(chan_ctx *c, int32_t *tile, int32_t *nchunks, int32_t *kchunk);
 

@@ -58,7 +58,7 @@ def test_launch_shapes_change_no_bits(mixed):
     p, x3, jac, inv, var = _strat_case(nP=(40, 20, 33))
     p = p.with_(mixed=mixed)
     ref = None
-    shapes = [(0, 0), (0, 1), (0, 5), (0, 31), (1, 0), (1, 1), (1, 7), (2, 0), (2, 3)]
+    shapes = [(0, 0), (0, 1), (0, 5), (0, 31), (1, 0), (1, 1), (1, 7), (2, 0), (2, 3), (3, 0), (3, 4)]
     for tile, nch in shapes:
         g = Channel(p, x3, jac, inv)
         g.set_buoyancy(0.1, 1.0)
@@ -82,7 +82,7 @@ def test_launch_shapes_change_no_bits(mixed):
 def test_launch_shape_rejects_bad_values():
     p, x3, jac, inv, var = _strat_case()
     g = Channel(p, x3, jac, inv)
-    for tile, nch in ((3, 0), (-1, 0), (0, -1), (0, 18)):
+    for tile, nch in ((4, 0), (-1, 0), (0, -1), (0, 18)):
         with pytest.raises(ChanError):
             g.set_launch(tile, nch)
     assert g.launch()[0] == 0
@@ -156,7 +156,7 @@ def test_ensemble_autotuner_leaves_states_unchanged():
     ms = e.tune(reps=2)
     assert ms > 0
     for sh in e.launch_shapes():
-        assert sh[0] in (0, 1, 2) and sh[1] >= 1
+        assert sh[0] in (0, 1, 2, 3) and sh[1] >= 1
     for g in a:
         g.step(8)
     assert e.step(8) == [0, 0, 0]
