@@ -349,17 +349,19 @@ def coarse_run(pc: ChanParams, x3, jac, inv, var, steps: int, cl: Closure | None
     rep = {"fallback_step": None, "reason": None, "plain_failed": None}
     try:
         if cl is None:
-            ch.step(first)
+            nonfinite = ch.step(first) != 0
             ch.time_avg_start()
             if sample_into is None:
-                ch.step(steps - first)
+                nonfinite = nonfinite or ch.step(steps - first) != 0
             else:
                 done = first
-                while done < steps:
+                while done < steps and not nonfinite:
                     n = min(sample_every, steps - done)
-                    ch.step(n)
+                    nonfinite = ch.step(n) != 0
                     done += n
                     sample_into.sample(ch, strides=(1, 1, 1), width=0)
+            if nonfinite:
+                rep = {"fallback_step": None, "reason": "blew up: non-finite state", "plain_failed": None}
         else:
             rep = run_with_fallback(ch, cl, first, check_every=check_every)
             ch.time_avg_start()

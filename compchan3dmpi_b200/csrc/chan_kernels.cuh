@@ -1974,13 +1974,14 @@ __global__ void k_selftest_pow07(const double *T, double *mine, double *libm, lo
 // advance, then per RK stage the stage kernel's CTAs and the wall kernel's
 // blocks, then on statistics steps the two statistics passes -- each phase a
 // number of units (one unit = one CTA's work of the kernel it replaces), and
-// lists all units of all members in one work list, members interleaved.  CTAs
-// take units from the list in order through an atomic counter.  A unit may
-// start once its member has completed every unit of its earlier phases: the
-// member's completion counter reaches the phase's `need`.  Units are taken in
-// list order and a unit only waits for units earlier in the list, which
-// running CTAs hold, so the launch always progresses; each wait is still
-// bounded (about a second), after which the CTA records the error and stops.
+// lists each member's units in order.  A CTA takes the next unit of any
+// member whose earlier work is complete -- its completion counter has reached
+// the unit's phase's `need` -- through that member's queue counter, so no CTA
+// waits behind a member that is not ready while another member has work.  A
+// member's units are taken in order and a unit only waits for units of its
+// member taken before it, which running CTAs hold, so the launch always
+// progresses; a CTA that finds no ready unit for about a second records the
+// error and stops.
 // Every member's arithmetic is the stand-alone kernels' code, so its results
 // are bit for bit those of chan_step.
 enum PKind { kPClock = 0, kPStage = 1, kPWall = 2, kPStatsPart = 3, kPStatsFin = 4 };
@@ -2008,11 +2009,13 @@ struct PItem {
 
 struct PPlan {
     const PPhase *phases;
-    const PItem *items;
-    long long nitems;
+    const PItem *items;         // every member's units in its own order, member after member
+    const long long *mfirst;    // [members] first unit of the member in items
+    const long long *mcount;    // [members] its number of units
+    int members;
     const KParams *kps;
     unsigned long long *done;   // [members] completed units
-    unsigned long long *next;   // work-list position
+    unsigned long long *taken;  // [members] units handed out (the member's queue position)
     int *err;                   // 1: a dependency wait gave up
     DevClock *clk;              // [members]
 };
@@ -2059,22 +2062,34 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
     long long *s_item = reinterpret_cast<long long *>(smem_raw + PS::body);
     int *s_ok = reinterpret_cast<int *>(s_item + 1);
     const int tid = threadIdx.x;
+    // rotating start so that the CTAs spread over the members
+    int start = (int)((blockIdx.x * 2654435761u) % (unsigned)plan.members);
     for (;;) {
         if (tid == 0) {
-            long long it = (long long)atomicAdd(plan.next, 1ull);
-            if (it < plan.nitems && *(volatile int *)plan.err) it = plan.nitems;   // after an error: stop
+            // take the next unit of the first member (from `start` on) whose
+            // earlier work is complete; units of one member are taken in order
+            long long it = -1;
             int ok = 1;
-            if (it < plan.nitems) {
-                const PPhase &F = plan.phases[plan.items[it].phase];
-                const unsigned long long *d = plan.done + F.member;
-                if (ld_acquire_u64(d) < F.need) {
-                    const unsigned long long t0 = global_ns();
-                    while (ld_acquire_u64(d) < F.need) {
-                        if (global_ns() - t0 > kDepWaitNs) { ok = 0; break; }
-                        __nanosleep(256);
+            unsigned long long t0 = 0;
+            for (;;) {
+                if (*(volatile int *)plan.err) break;
+                bool left = false;
+                for (int r = 0; r < plan.members && it < 0; r++) {
+                    const int m = (start + r) % plan.members;
+                    unsigned long long u = *(volatile unsigned long long *)(plan.taken + m);
+                    while (u < (unsigned long long)plan.mcount[m]) {
+                        left = true;
+                        const long long cand = plan.mfirst[m] + (long long)u;
+                        if (ld_acquire_u64(plan.done + m) < plan.phases[plan.items[cand].phase].need) break;
+                        const unsigned long long got = atomicCAS(plan.taken + m, u, u + 1);
+                        if (got == u) { it = cand; start = m; break; }
+                        u = got;   // another CTA took it: look at the member's next unit
                     }
                 }
-                if (!ok) atomicExch(plan.err, 1);
+                if (it >= 0 || !left) break;
+                if (t0 == 0) t0 = global_ns();
+                else if (global_ns() - t0 > kDepWaitNs) { ok = 0; atomicExch(plan.err, 1); break; }
+                __nanosleep(256);
             }
             *s_item = it;
             *s_ok = ok;
@@ -2083,7 +2098,7 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
         const long long it = *s_item;
         const int ok = *s_ok;
         __syncthreads();
-        if (it >= plan.nitems || !ok) break;
+        if (it < 0 || !ok) break;
         const PItem I = plan.items[it];
         const PPhase &F = plan.phases[I.phase];
         const KParams &P = plan.kps[F.kp];
