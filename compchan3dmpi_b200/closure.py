@@ -514,6 +514,9 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
     log(json.dumps({"phase": "coarse plain (calibration seed)", "wall_s": plain_cal["wall_s"],
                     "samples": craw.count,
                     "errors": _errors(plain_cal["stats"], dns_c) if plain_cal["stats"] else None}))
+    if plain_cal["stats"] is None:
+        raise RuntimeError(f"the plain coarse run failed ({plain_cal['report']['reason']}): "
+                           "no deficit to train on; try a smaller CFL or a finer coarse grid")
     # what the coarse solver misses: rho <u'w'> deficit at the coarse points
     uw_d = np.asarray(dns_c["uw"]) * rho_d[::kst]
     uw_c = np.asarray(plain_cal["stats"]["uw"]) * rho_d[::kst]

@@ -1974,10 +1974,12 @@ __global__ void k_selftest_pow07(const double *T, double *mine, double *libm, lo
 // advance, then per RK stage the stage kernel's CTAs and the wall kernel's
 // blocks, then on statistics steps the two statistics passes -- each phase a
 // number of units (one unit = one CTA's work of the kernel it replaces), and
-// lists each member's units in order.  A CTA takes the next unit of any
-// member whose earlier work is complete -- its completion counter has reached
-// the unit's phase's `need` -- through that member's queue counter, so no CTA
-// waits behind a member that is not ready while another member has work.  A
+// lists each member's units in order.  A CTA takes the next unit of a member
+// whose earlier work is complete -- its completion counter has reached the
+// unit's phase's `need` -- through that member's queue counter, choosing among
+// the ready members the one furthest behind, so no CTA waits behind a member
+// that is not ready while another member has work, and the members advance
+// together.  A
 // member's units are taken in order and a unit only waits for units of its
 // member taken before it, which running CTAs hold, so the launch always
 // progresses; a CTA that finds no ready unit for about a second records the
@@ -2007,13 +2009,19 @@ struct PItem {
     int unit;
 };
 
+// The members' parameter records of the running persistent block, in constant
+// memory: a stage body reads its record's fields many times, and from the
+// constant cache those reads are cheap where global memory would put a load
+// and its latency on each.  A block's graph copies its records here first.
+constexpr int kEnsKps = 64;
+__constant__ KParams c_ens_kps[kEnsKps];
+
 struct PPlan {
     const PPhase *phases;
     const PItem *items;         // every member's units in its own order, member after member
     const long long *mfirst;    // [members] first unit of the member in items
     const long long *mcount;    // [members] its number of units
     int members;
-    const KParams *kps;
     unsigned long long *done;   // [members] completed units
     unsigned long long *taken;  // [members] units handed out (the member's queue position)
     int *err;                   // 1: a dependency wait gave up
@@ -2062,8 +2070,6 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
     long long *s_item = reinterpret_cast<long long *>(smem_raw + PS::body);
     int *s_ok = reinterpret_cast<int *>(s_item + 1);
     const int tid = threadIdx.x;
-    // rotating start so that the CTAs spread over the members
-    int start = (int)((blockIdx.x * 2654435761u) % (unsigned)plan.members);
     for (;;) {
         if (tid == 0) {
             // take the next unit of the first member (from `start` on) whose
@@ -2073,20 +2079,27 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
             unsigned long long t0 = 0;
             for (;;) {
                 if (*(volatile int *)plan.err) break;
+                // among the members whose next unit is ready, the one furthest
+                // behind (fewest units taken, as a fraction of its block): the
+                // members advance together, as the graph of their kernels does
                 bool left = false;
-                for (int r = 0; r < plan.members && it < 0; r++) {
-                    const int m = (start + r) % plan.members;
-                    unsigned long long u = *(volatile unsigned long long *)(plan.taken + m);
-                    while (u < (unsigned long long)plan.mcount[m]) {
-                        left = true;
-                        const long long cand = plan.mfirst[m] + (long long)u;
-                        if (ld_acquire_u64(plan.done + m) < plan.phases[plan.items[cand].phase].need) break;
-                        const unsigned long long got = atomicCAS(plan.taken + m, u, u + 1);
-                        if (got == u) { it = cand; start = m; break; }
-                        u = got;   // another CTA took it: look at the member's next unit
-                    }
+                int best = -1;
+                unsigned long long bu = 0;
+                double bp = 2.0;
+                for (int m = 0; m < plan.members; m++) {
+                    const unsigned long long u = *(volatile unsigned long long *)(plan.taken + m);
+                    if (u >= (unsigned long long)plan.mcount[m]) continue;
+                    left = true;
+                    const long long cand = plan.mfirst[m] + (long long)u;
+                    if (ld_acquire_u64(plan.done + m) < plan.phases[plan.items[cand].phase].need) continue;
+                    const double pr = (double)u / (double)plan.mcount[m];
+                    if (pr < bp) { bp = pr; best = m; bu = u; }
                 }
-                if (it >= 0 || !left) break;
+                if (best >= 0) {
+                    if (atomicCAS(plan.taken + best, bu, bu + 1) == bu) { it = plan.mfirst[best] + (long long)bu; break; }
+                    continue;   // another CTA took it: look again
+                }
+                if (!left) break;
                 if (t0 == 0) t0 = global_ns();
                 else if (global_ns() - t0 > kDepWaitNs) { ok = 0; atomicExch(plan.err, 1); break; }
                 __nanosleep(256);
@@ -2101,7 +2114,7 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
         if (it < 0 || !ok) break;
         const PItem I = plan.items[it];
         const PPhase &F = plan.phases[I.phase];
-        const KParams &P = plan.kps[F.kp];
+        const KParams &P = c_ens_kps[F.kp];
         switch (F.kind) {
         case kPClock:
             if (tid == 0) {

@@ -1673,6 +1673,9 @@ std::string persistent_blocker(const chan_ensemble *e)
         if (c->closure_on) return "a member runs with the learned closure";
         if (c->tile != CHAN_TILE_32x8 && c->tile != CHAN_TILE_16x16) return "a member uses a tile of other than 256 threads";
     }
+    long long recs = 0;
+    for (chan_ctx *c : e->m) recs += c->nstage;
+    if (recs > chan::kEnsKps) return "more parameter records than the persistent kernel's constant memory holds";
     return "";
 }
 
@@ -1793,10 +1796,14 @@ int build_persistent(chan_ensemble *e)
 
     chan::PPlan plan{};
     plan.phases = e->dph; plan.items = e->ditems; plan.mfirst = e->dmq; plan.mcount = e->dmq + n;
-    plan.members = (int)n; plan.kps = e->dkps;
+    plan.members = (int)n;
     plan.done = e->dcnt; plan.taken = e->dcnt + n; plan.err = e->derr; plan.clk = e->dclk;
+    void *ckps = nullptr;
+    EK(e, cudaGetSymbolAddress(&ckps, chan::c_ens_kps));
     EK(e, cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
-    cudaError_t r = cudaMemsetAsync(e->dcnt, 0, 2 * n * sizeof(unsigned long long), e->origin);
+    cudaError_t r = cudaMemcpyAsync(ckps, e->dkps, kps.size() * sizeof(chan::KParams), cudaMemcpyDeviceToDevice,
+                                    e->origin);
+    if (r == cudaSuccess) r = cudaMemsetAsync(e->dcnt, 0, 2 * n * sizeof(unsigned long long), e->origin);
     if (r == cudaSuccess) {
         if (mixed)
             chan::k_ensemble<true><<<e->pgrid, 256, smem, e->origin>>>(plan);

@@ -470,9 +470,12 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms);
  *   clock advance -- members interleaved; a unit starts once its member has
  *   completed its earlier work, which per-member device counters track, and
  *   each such wait is bounded (about a second).  The block is one graph of
- *   two nodes (counter reset, the launch).  It needs members of one
- *   precision, without the closure, on the 32x8 or 16x16 tile; otherwise the
- *   graph mode is used and chan_ensemble_get_mode says why.
+ *   three nodes (the members' parameter records into constant memory, counter
+ *   reset, the launch).  It needs members of one precision, without the
+ *   closure, on the 32x8 or 16x16 tile, at most 64 parameter records (one per
+ *   RK stage per member); otherwise the graph mode is used and
+ *   chan_ensemble_get_mode says why.  The records' constant memory is one per
+ *   device: two ensembles must not step concurrently in persistent mode.
  * CHAN_ENSEMBLE_GRAPH: one graph of every member's kernels, one branch per
  *   member on its own stream.
  * Either way each member's results are bit for bit those of chan_step.
