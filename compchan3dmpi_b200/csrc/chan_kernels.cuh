@@ -2008,16 +2008,14 @@ __global__ void k_selftest_pow07(const double *T, double *mine, double *libm, lo
 // advance, then per RK stage the stage kernel's CTAs and the wall kernel's
 // blocks, then on statistics steps the two statistics passes -- each phase a
 // number of units (one unit = one CTA's work of the kernel it replaces), and
-// lists each member's units in order.  A CTA takes the next unit of a member
-// whose earlier work is complete -- its completion counter has reached the
-// unit's phase's `need` -- through that member's queue counter, choosing among
-// the ready members the one furthest behind, so no CTA waits behind a member
-// that is not ready while another member has work, and the members advance
-// together.  A
-// member's units are taken in order and a unit only waits for units of its
-// member taken before it, which running CTAs hold, so the launch always
-// progresses; a CTA that finds no ready unit for about a second records the
-// error and stops.
+// lists all units of all members in one work list, members interleaved phase
+// by phase.  CTAs take units from the list in order through an atomic
+// counter.  A unit may start once its member has completed every unit of its
+// earlier phases: the member's completion counter reaches the phase's `need`.
+// Units are taken in list order and a unit only waits for units earlier in the
+// list, which running CTAs hold, so the launch always progresses; each wait is
+// still bounded (about a second), after which the CTA records the error and
+// stops.
 // Every member's arithmetic is the stand-alone kernels' code, so its results
 // are bit for bit those of chan_step.
 enum PKind { kPClock = 0, kPStage = 1, kPWall = 2, kPStatsPart = 3, kPStatsFin = 4 };
@@ -2052,14 +2050,15 @@ __constant__ KParams c_ens_kps[kEnsKps];
 
 struct PPlan {
     const PPhase *phases;
-    const PItem *items;         // every member's units in its own order, member after member
-    const long long *mfirst;    // [members] first unit of the member in items
-    const long long *mcount;    // [members] its number of units
-    int members;
+    const PItem *items;         // the work list: members' units interleaved phase by phase
+    long long nitems;
     unsigned long long *done;   // [members] completed units
-    unsigned long long *taken;  // [members] units handed out (the member's queue position)
+    unsigned long long *next;   // work-list position
     int *err;                   // 1: a dependency wait gave up
     DevClock *clk;              // [members]
+#ifdef CHAN_PERSIST_GLOBAL_KPS
+    const KParams *kps;
+#endif
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
@@ -2106,37 +2105,22 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
-            // take the next unit of the first member (from `start` on) whose
-            // earlier work is complete; units of one member are taken in order
-            long long it = -1;
+            // the next unit of the work list; wait (bounded) until its member has
+            // completed the units of its earlier phases
+            long long it = (long long)atomicAdd(plan.next, 1ull);
+            if (it < plan.nitems && *(volatile int *)plan.err) it = plan.nitems;   // after an error: stop
             int ok = 1;
-            unsigned long long t0 = 0;
-            for (;;) {
-                if (*(volatile int *)plan.err) break;
-                // among the members whose next unit is ready, the one furthest
-                // behind (fewest units taken, as a fraction of its block): the
-                // members advance together, as the graph of their kernels does
-                bool left = false;
-                int best = -1;
-                unsigned long long bu = 0;
-                double bp = 2.0;
-                for (int m = 0; m < plan.members; m++) {
-                    const unsigned long long u = *(volatile unsigned long long *)(plan.taken + m);
-                    if (u >= (unsigned long long)plan.mcount[m]) continue;
-                    left = true;
-                    const long long cand = plan.mfirst[m] + (long long)u;
-                    if (ld_acquire_u64(plan.done + m) < plan.phases[plan.items[cand].phase].need) continue;
-                    const double pr = (double)u / (double)plan.mcount[m];
-                    if (pr < bp) { bp = pr; best = m; bu = u; }
+            if (it < plan.nitems) {
+                const PPhase &F = plan.phases[plan.items[it].phase];
+                const unsigned long long *d = plan.done + F.member;
+                if (ld_acquire_u64(d) < F.need) {
+                    const unsigned long long t0 = global_ns();
+                    while (ld_acquire_u64(d) < F.need) {
+                        if (global_ns() - t0 > kDepWaitNs) { ok = 0; break; }
+                        __nanosleep(256);
+                    }
                 }
-                if (best >= 0) {
-                    if (atomicCAS(plan.taken + best, bu, bu + 1) == bu) { it = plan.mfirst[best] + (long long)bu; break; }
-                    continue;   // another CTA took it: look again
-                }
-                if (!left) break;
-                if (t0 == 0) t0 = global_ns();
-                else if (global_ns() - t0 > kDepWaitNs) { ok = 0; atomicExch(plan.err, 1); break; }
-                __nanosleep(256);
+                if (!ok) atomicExch(plan.err, 1);
             }
             *s_item = it;
             *s_ok = ok;
@@ -2145,10 +2129,14 @@ __global__ void __launch_bounds__(256, PersistShape<MIXED>::minb) k_ensemble(con
         const long long it = *s_item;
         const int ok = *s_ok;
         __syncthreads();
-        if (it < 0 || !ok) break;
+        if (it >= plan.nitems || !ok) break;
         const PItem I = plan.items[it];
         const PPhase &F = plan.phases[I.phase];
+#ifdef CHAN_PERSIST_GLOBAL_KPS
+        const KParams &P = plan.kps[F.kp];   // measurement variant: records in global memory
+#else
         const KParams &P = c_ens_kps[F.kp];
+#endif
         switch (F.kind) {
         case kPClock:
             if (tid == 0) {

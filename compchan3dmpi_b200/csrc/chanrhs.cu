@@ -1589,15 +1589,14 @@ struct chan_ensemble {
     double last_ms = 0.0;             // device time of the last call's graph replays (CUDA events)
     std::string err;
     // persistent mode: one persistent kernel per block of L steps (k_ensemble)
-    int mode = CHAN_ENSEMBLE_PERSISTENT;   // requested mode
+    int mode = CHAN_ENSEMBLE_GRAPH;        // requested mode
     bool persistent = false;               // the captured graph holds the persistent kernel
     std::string fallback;                  // why the requested persistent mode fell back
     chan::PPhase *dph = nullptr;
     chan::PItem *ditems = nullptr;
     chan::KParams *dkps = nullptr;
     CUtensorMap *dmaps = nullptr;
-    unsigned long long *dcnt = nullptr;    // [n] completed units per member, then [n] units taken
-    long long *dmq = nullptr;              // [n] first unit of each member in the work list, then [n] unit counts
+    unsigned long long *dcnt = nullptr;    // [n] completed units per member, then the work-list position
     int *derr = nullptr, *herr = nullptr;
     size_t cap_ph = 0, cap_items = 0, cap_kps = 0, cap_maps = 0;
     long long nitems = 0;
@@ -1752,14 +1751,10 @@ int build_persistent(chan_ensemble *e)
         ph.insert(ph.end(), per[i].begin(), per[i].end());
         maxp = std::max(maxp, per[i].size());
     }
-    std::vector<long long> mfirst(n), mcount(n);
-    for (size_t i = 0; i < n; i++) {
-        mfirst[i] = (long long)items.size();
-        for (size_t q = 0; q < per[i].size(); q++)
-            for (int u = 0; u < per[i][q].units; u++) items.push_back({(int)(first[i] + q), u});
-        mcount[i] = (long long)items.size() - mfirst[i];
-    }
-    (void)maxp;
+    for (size_t q = 0; q < maxp; q++)
+        for (size_t i = 0; i < n; i++)
+            if (q < per[i].size())
+                for (int u = 0; u < per[i][q].units; u++) items.push_back({(int)(first[i] + q), u});
     EK(e, ensure_dev(&e->dmaps, &e->cap_maps, maps.size()));
     for (auto &f : ph)
         if (f.kind == chan::kPStage) f.tm = e->dmaps + f.kp;
@@ -1771,10 +1766,7 @@ int build_persistent(chan_ensemble *e)
     EK(e, ensure_dev(&e->dph, &e->cap_ph, ph.size()));
     EK(e, ensure_dev(&e->ditems, &e->cap_items, items.size()));
     EK(e, ensure_dev(&e->dkps, &e->cap_kps, kps.size()));
-    if (!e->dcnt) EK(e, cudaMalloc((void **)&e->dcnt, 2 * n * sizeof(unsigned long long)));
-    if (!e->dmq) EK(e, cudaMalloc((void **)&e->dmq, 2 * n * sizeof(long long)));
-    EK(e, cudaMemcpyAsync(e->dmq, mfirst.data(), n * sizeof(long long), cudaMemcpyHostToDevice, e->origin));
-    EK(e, cudaMemcpyAsync(e->dmq + n, mcount.data(), n * sizeof(long long), cudaMemcpyHostToDevice, e->origin));
+    if (!e->dcnt) EK(e, cudaMalloc((void **)&e->dcnt, (n + 1) * sizeof(unsigned long long)));
     if (!e->derr) EK(e, cudaMalloc((void **)&e->derr, sizeof(int)));
     if (!e->herr) EK(e, cudaMallocHost((void **)&e->herr, sizeof(int)));
     EK(e, cudaMemcpyAsync(e->dmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, e->origin));
@@ -1795,15 +1787,17 @@ int build_persistent(chan_ensemble *e)
     e->pgrid = std::max(1, occ) * sms;
 
     chan::PPlan plan{};
-    plan.phases = e->dph; plan.items = e->ditems; plan.mfirst = e->dmq; plan.mcount = e->dmq + n;
-    plan.members = (int)n;
-    plan.done = e->dcnt; plan.taken = e->dcnt + n; plan.err = e->derr; plan.clk = e->dclk;
+    plan.phases = e->dph; plan.items = e->ditems; plan.nitems = e->nitems;
+    plan.done = e->dcnt; plan.next = e->dcnt + n; plan.err = e->derr; plan.clk = e->dclk;
+#ifdef CHAN_PERSIST_GLOBAL_KPS
+    plan.kps = e->dkps;
+#endif
     void *ckps = nullptr;
     EK(e, cudaGetSymbolAddress(&ckps, chan::c_ens_kps));
     EK(e, cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
     cudaError_t r = cudaMemcpyAsync(ckps, e->dkps, kps.size() * sizeof(chan::KParams), cudaMemcpyDeviceToDevice,
                                     e->origin);
-    if (r == cudaSuccess) r = cudaMemsetAsync(e->dcnt, 0, 2 * n * sizeof(unsigned long long), e->origin);
+    if (r == cudaSuccess) r = cudaMemsetAsync(e->dcnt, 0, (n + 1) * sizeof(unsigned long long), e->origin);
     if (r == cudaSuccess) {
         if (mixed)
             chan::k_ensemble<true><<<e->pgrid, 256, smem, e->origin>>>(plan);
@@ -2187,7 +2181,6 @@ void chan_ensemble_free(chan_ensemble *e)
     if (e->dkps) cudaFree(e->dkps);
     if (e->dmaps) cudaFree(e->dmaps);
     if (e->dcnt) cudaFree(e->dcnt);
-    if (e->dmq) cudaFree(e->dmq);
     if (e->derr) cudaFree(e->derr);
     if (e->herr) cudaFreeHost(e->herr);
     if (e->origin) cudaStreamDestroy(e->origin);

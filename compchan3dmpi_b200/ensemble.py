@@ -4,10 +4,10 @@ parameter sweep they are built for.
 ``Ensemble`` wraps chan_ensemble_* (include/chanrhs.h): a block of L steps
 of every member (L = least common multiple of the members' istat) is
 captured once into a CUDA graph and replayed.  By default that graph holds
-one persistent kernel which runs every member's work units from one work
-list, ordered by per-member device counters with bounded waits
-(``mode="persistent"``); ``mode="graph"`` captures every member's kernels
-instead, one branch per member on its own stream.  Results are bit for bit
+every member's kernels, one branch per member on its own stream
+(``mode="graph"``); ``mode="persistent"`` captures instead one persistent
+kernel which runs every member's work units from one work list, ordered by
+per-member device counters with bounded waits.  Results are bit for bit
 those of stepping each member alone.  ``Ensemble.tune`` runs the
 launch-shape autotuner.
 
@@ -74,7 +74,7 @@ class Ensemble:
              "persistent-stall-test": _lib.CHAN_ENSEMBLE_PERSISTENT_STALL_TEST}
 
     def set_mode(self, mode: str):
-        """"persistent" (default), "graph", or "persistent-stall-test" (host-side
+        """"graph" (default), "persistent", or "persistent-stall-test" (host-side
         fault injection: a dependency that is never met, for tests)."""
         r = self.L.chan_ensemble_set_mode(self._h, self.MODES[mode])
         if r != 0:

@@ -430,9 +430,9 @@ void chan_free(chan_ctx *c);
  * their own grids, physics, wall BCs and precision -- stepped together.
  * Every member keeps its own buffers and stream.  A block of L steps of all
  * members (L = least common multiple of their istat) is captured once into
- * one CUDA graph and replayed: by default one persistent kernel that runs
- * all members' work (chan_ensemble_set_mode below), else one branch of
- * kernels per member, run concurrently.  Each member's results are bit for bit those of
+ * one CUDA graph and replayed: by default one branch of kernels per member,
+ * run concurrently, or one persistent kernel that runs all members' work
+ * (chan_ensemble_set_mode below).  Each member's results are bit for bit those of
  * chan_step on that member alone.  A context belongs to one ensemble at most;
  * members may still be used on their own between ensemble calls. */
 typedef struct chan_ensemble chan_ensemble;
@@ -464,7 +464,7 @@ int chan_ensemble_step(chan_ensemble *e, int32_t nsteps, int32_t *status);
 int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms);
 
 /* How a block of L steps runs (no reference counterpart).
- * CHAN_ENSEMBLE_PERSISTENT (the default): one persistent kernel per block.
+ * CHAN_ENSEMBLE_PERSISTENT: one persistent kernel per block.
  *   It walks one work list of every member's units -- the CTAs of each RK
  *   stage, of each wall-BC pass and of the statistics passes, and the step's
  *   clock advance -- members interleaved; a unit starts once its member has
@@ -476,8 +476,8 @@ int chan_ensemble_tune(chan_ensemble *e, int32_t reps, double *best_ms);
  *   RK stage per member); otherwise the graph mode is used and
  *   chan_ensemble_get_mode says why.  The records' constant memory is one per
  *   device: two ensembles must not step concurrently in persistent mode.
- * CHAN_ENSEMBLE_GRAPH: one graph of every member's kernels, one branch per
- *   member on its own stream.
+ * CHAN_ENSEMBLE_GRAPH (the default, faster on the stratified sweep): one graph
+ *   of every member's kernels, one branch per member on its own stream.
  * Either way each member's results are bit for bit those of chan_step.
  * CHAN_ENSEMBLE_PERSISTENT_STALL_TEST: persistent, with member 0's first stage
  *   made to wait for work that never completes (host-side fault injection

@@ -238,6 +238,7 @@ def test_persistent_ensemble_matches_members_alone(precision):
     solo = [_open(s) for s in specs]
     ens_m = [_open(s) for s in specs]
     e = Ensemble(ens_m)
+    e.set_mode("persistent")
     plan = [13, 5, "avg", 12]
     for item in plan:
         if item == "avg":
@@ -264,6 +265,7 @@ def test_persistent_ensemble_matches_members_alone(precision):
 def test_persistent_mode_falls_back_for_mixed_precisions_and_graph_mode_matches():
     specs = _members()            # FP64 and mixed members together
     e = Ensemble([_open(s) for s in specs])
+    e.set_mode("persistent")
     e.step(6)
     assert e.mode_in_use() == ("graph", "members of both precisions")
     e.close()
@@ -271,7 +273,7 @@ def test_persistent_mode_falls_back_for_mixed_precisions_and_graph_mode_matches(
     a = [_open(s) for s in fp]
     b = [_open(s) for s in fp]
     ea, eb = Ensemble(a), Ensemble(b)
-    eb.set_mode("graph")
+    ea.set_mode("persistent")
     ea.step(12)
     eb.step(12)
     assert ea.mode_in_use()[0] == "persistent" and eb.mode_in_use()[0] == "graph"
@@ -315,6 +317,7 @@ def test_persistent_member_blowup_is_reported_for_that_member_only():
     bad = Channel(p.with_(dt=p.dt * 400), x3, jac, inv)
     bad.init_sol_v(var)
     e = Ensemble(good + [bad])
+    e.set_mode("persistent")
     st = e.step(12)
     assert e.mode_in_use()[0] == "persistent"
     assert st[0] == 0 and st[1] in (_lib.CHAN_BLOWUP, _lib.CHAN_NONFINITE)

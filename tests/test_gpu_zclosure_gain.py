@@ -8,20 +8,21 @@ pytestmark = pytest.mark.gpu
 
 def test_trained_closure_lowers_the_coarse_run_error():
     """The whole closure pipeline on a small case, and what the trained network
-    gains over the coarse method without it.  A small DNS (48x33x48 from a
-    seeded smooth perturbation) is sampled through the width-4 filter; a plain
-    coarse run (12x17x16, 4x / 2x / 3x coarser) gives its Reynolds-shear-stress
-    deficit against the DNS; the network trains on the filtered subgrid fluxes
-    plus that deficit; its magnitude is picked by coarse runs.  Stated metric:
-    the sum of the relative errors of Cf and of the <u'w'> peak against the
-    DNS, over the second half of a coarse run from a second seed.  With the
-    closure it must be lower than without it."""
+    gains over the coarse method without it.  A small DNS (128x129x96 from a
+    seeded smooth perturbation, 20,000 steps) is sampled through the width-4
+    filter; a plain coarse run on the production coarse grid (64x65x64, 6,000
+    steps) gives its Reynolds-shear-stress deficit against the DNS and its own
+    closure inputs; the network trains on both; its magnitude is picked by
+    coarse runs from one seed.  Stated metric: the sum of the relative errors
+    of Cf and of the <u'w'> peak against the DNS, over the second half of a
+    coarse run from a second seed.  With the closure it must be lower than
+    without it (measured 0.63 against 0.76)."""
     from compchan3dmpi_b200.closure import experiment
-    res, params, norm = experiment(dns_grid=(48, 48, 33), coarse_grid=(12, 16, 17), spinup=3000, snapshots=20,
-                                   snap_every=50, coarse_steps=2000, epochs=10, batch=4096, rec_every=100,
-                                   alphas=(0.5, 1.0, 2.0), log=lambda s: None)
+    res, params, norm = experiment(dns_grid=(128, 96, 129), coarse_grid=(64, 64, 65), spinup=20000, snapshots=20,
+                                   snap_every=100, coarse_steps=6000, epochs=10, batch=4096, rec_every=200,
+                                   coarse_snapshots=20, alphas=(0.5, 1.0, 2.0), log=lambda s: None)
     runs = res["coarse"]["runs"]
-    assert res["coarse"]["alpha"] is not None, res["coarse"]["calibration"]
+    assert res["coarse"]["alpha"] is not None, res["coarse"]["training_sets"]
     e_plain, e_cl = runs["plain"]["errors_vs_dns"], runs["closure"]["errors_vs_dns"]
     assert runs["closure"]["report"]["fallback_step"] is None
     m_plain = e_plain["Cf"] + e_plain["uw_peak"]
