@@ -193,13 +193,15 @@ struct SlotT {
     const R *U, *V, *W, *T;
 };
 
-// pressure at box point b.  With FP64 rings PR is the ring's pressure slot;
-// with float rings there is no pressure slot, PR is the density slot and p is
-// rho*T/(gama*Ma^2) formed on the spot (one multiply against two shared loads).
-template <typename R>
+// pressure at box point b.  With a pressure ring (PRING) PR is the ring's
+// pressure slot; without one PR is the density slot and p is rho*T/(gama*Ma^2)
+// formed on the spot (one multiply against two shared loads).  On interior
+// planes both give the same bits in FP64: the ring's p is formed by the same
+// two products of the same values.
+template <typename R, bool PRING = (sizeof(R) == 8)>
 __device__ __forceinline__ R pres_at(const FluxC<R> &C, const SlotT<R> &s, const R *PR, int b)
 {
-    if constexpr (sizeof(R) == 4) return (PR[b] * s.T[b]) * C.inv_gM2;
+    if constexpr (!PRING) return (PR[b] * s.T[b]) * C.inv_gM2;
     else return PR[b];
 }
 
@@ -259,7 +261,7 @@ __device__ __forceinline__ void gd_point(const FluxC<R> &C, R mu, R pr, R u0, R 
 // The flux helpers below take plane t's primitives from the ring slot s, plane
 // t+1's from sp, and plane t-1's values at point b as scalars (um, vm, wm),
 // which the caller keeps outside the ring.
-template <int BX, typename R>
+template <int BX, typename R, bool PRING = (sizeof(R) == 8)>
 __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, R um, R wm, const SlotT<R> &sp,
                                         const R *MU, const R *PR, int b, R czt, R f[4])
 {
@@ -271,10 +273,10 @@ __device__ __forceinline__ void visc_fx(const FluxC<R> &C, const SlotT<R> &s, R 
     const R Tx = (s.T[b + 1] - s.T[b - 1]) * C.hdx;
     const R uz = (sp.U[b] - um) * czt;
     const R wz = (sp.W[b] - wm) * czt;
-    fd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wx, uz, Tx, f);
+    fd_point(C, MU[b], pres_at<R, PRING>(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wx, uz, Tx, f);
 }
 
-template <int BX, typename R>
+template <int BX, typename R, bool PRING = (sizeof(R) == 8)>
 __device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, R vm, R wm, const SlotT<R> &sp,
                                         const R *MU, const R *PR, int b, R czt, R g[4])
 {
@@ -286,12 +288,12 @@ __device__ __forceinline__ void visc_fy(const FluxC<R> &C, const SlotT<R> &s, R 
     const R Ty = (s.T[b + BX] - s.T[b - BX]) * C.hdy;
     const R vz = (sp.V[b] - vm) * czt;
     const R wz = (sp.W[b] - wm) * czt;
-    gd_point(C, MU[b], pres_at(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wy, vz, Ty, g);
+    gd_point(C, MU[b], pres_at<R, PRING>(C, s, PR, b), s.U[b], s.V[b], s.W[b], ux, vy, wz, vx, uy, wy, vz, Ty, g);
 }
 
 // fD and gD together at one point: they share eight gradients, the shear
 // stress mu*(dv/dx+du/dy) (fD3 = gD2) and p + 2/3*mu*div.
-template <int BX, typename R>
+template <int BX, typename R, bool PRING = (sizeof(R) == 8)>
 __device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, R um, R vm, R wm, const SlotT<R> &sp,
                                          const R *MU, const R *PR, int b, R czt, R f[4], R g[4])
 {
@@ -306,7 +308,7 @@ __device__ __forceinline__ void visc_fxy(const FluxC<R> &C, const SlotT<R> &s, R
     const R uz = (sp.U[b] - um) * czt;
     const R vz = (sp.V[b] - vm) * czt;
     const R wz = (sp.W[b] - wm) * czt;
-    const R mu = MU[b], pr = pres_at(C, s, PR, b);
+    const R mu = MU[b], pr = pres_at<R, PRING>(C, s, PR, b);
     const R u0 = s.U[b], v0 = s.V[b], w0 = s.W[b];
     fd_point(C, mu, pr, u0, v0, w0, ux, vy, wz, vx, uy, wx, uz, Tx, f);
     gd_point(C, mu, pr, u0, v0, w0, ux, vy, wz, vx, uy, wy, vz, Ty, g);
@@ -433,10 +435,20 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
 template <int TI, int TJ, typename R>
 struct StageShape {
     static constexpr int BX = TI + 4, BY = TJ + 4, NB = BX * BY, NT = TI * TJ;
-    static constexpr int NFX = TJ * (TI + 2), NGY = (TJ + 2) * TI;
+    // FP64 rings with 32-wide tiles: the own point's RK base arrives by a bulk
+    // copy of the tile (tma_base); the room for it comes from forming p from
+    // rho and T (no p ring) and exchanging fD along x by warp shuffles (a warp
+    // is a row of the tile), which leaves only the two halo columns in sF.
+#ifdef CHAN_TMA_BASE
+    static constexpr bool tma_base = sizeof(R) == 8 && TI == 32;
+#else
+    static constexpr bool tma_base = false;
+#endif
+    static constexpr bool fx_shfl = tma_base;
+    static constexpr int NFX = fx_shfl ? 2 * TJ : TJ * (TI + 2), NGY = (TJ + 2) * TI;
     // float rings keep mu only and form p from rho and T where it is used;
-    // FP64 rings keep (mu, p)
-    static constexpr bool p_ring = sizeof(R) == 8;
+    // FP64 rings keep (mu, p) unless the RK base takes the room
+    static constexpr bool p_ring = sizeof(R) == 8 && !tma_base;
     static constexpr int MPW = p_ring ? 2 : 1;                       // words per box point in the (mu, p) ring
     // one Q slot: the 5-variable box of one plane, rounded up to 128 bytes
     // (the alignment of a bulk tensor copy's shared-memory destination)
@@ -450,12 +462,14 @@ struct StageShape {
     // float rings leave room to stage the RK base of every thread's own point
     // (double) by cp.async; the FP64 rings do not fit it beside two CTAs per SM
     static constexpr bool prefetch_base = sizeof(R) == 4;
-    static constexpr size_t base_off = (q_bytes + sizeof(R) * (size_t)(pr_words + mp_words + fg_words) + 15) / 16 * 16;
+    static constexpr bool base_slot = prefetch_base || tma_base;
+    // the base slot is a bulk-copy destination: 128-byte aligned
+    static constexpr size_t base_off = (q_bytes + sizeof(R) * (size_t)(pr_words + mp_words + fg_words) + 127) / 128 * 128;
     // plane t-1 values (u or v, and w) of the halo-flux lanes' points, by lane
     static constexpr int NHL = 32 + 2 * TI;
-    static constexpr size_t hl_off = base_off + (prefetch_base ? sizeof(double) * 5 * (size_t)NT : 0);
+    static constexpr size_t hl_off = base_off + (base_slot ? sizeof(double) * 5 * (size_t)NT : 0);
     static constexpr size_t bar_off = (hl_off + sizeof(R) * 2 * (size_t)NHL + 7) / 8 * 8;
-    static constexpr size_t bytes = bar_off + 3 * sizeof(unsigned long long) + 2 * sizeof(int);
+    static constexpr size_t bytes = bar_off + 4 * sizeof(unsigned long long) + 2 * sizeof(int);
     // resident CTAs per SM the register budget is sized for: 128 (FP64) or 80
     // (float) registers per thread at 256 threads, but never more CTAs than
     // the 228 KB of shared memory per SM holds (1 KB of it reserved per CTA)
@@ -573,8 +587,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
 // was written earlier in the same launch: coherent loads instead of the
 // read-only path, and a proxy fence before the first box copy.
 template <int TI, int TJ, typename QI, typename QO, typename R, int BUOYM, bool PERSIST>
-__device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *tmq, int bx, int by, int bz, int tx,
-                                           int ty, unsigned char *smem_raw)
+__device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *tmq, const CUtensorMap *tmb, int bx,
+                                           int by, int bz, int tx, int ty, unsigned char *smem_raw)
 {
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
@@ -595,7 +609,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     R *sH = reinterpret_cast<R *>(smem_raw + S::hl_off);                // [2][NHL]
     // (the 8-byte rounding is a no-op: bar_off is a multiple of 8)
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(reinterpret_cast<size_t>(smem_raw + S::bar_off) & ~(size_t)7);   // [3]
-    int *sflag = reinterpret_cast<int *>(bar + 3);   // [0] the CTA leaves at once, [1] Q slots with a copy in flight
+    int *sflag = reinterpret_cast<int *>(bar + 4);   // [0] the CTA leaves at once, [1] slots with a copy in flight
     const FluxC<R> &C = fluxc<R>(P);
     // the state pointers are read from the parameter space at each use: held
     // in registers across the kernel they cost spills
@@ -614,8 +628,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             sflag[0] = 1;
             atomicExch(&P.status->stall, 2);
         }
-        if (TMA) {
-            for (int s = 0; s < 3; s++) mbar_init_one(&bar[s]);
+        if (TMA || S::tma_base) {
+            for (int s = 0; s < 4; s++) mbar_init_one(&bar[s]);
             fence_mbar_init();
         }
     }
@@ -658,7 +672,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     };
     // wait for Q slot s; false if the copy did not complete in time
     auto wait_slot = [&](int s) -> bool {
-        if (!TMA) return true;
+        if (s < 3 ? !TMA : !S::tma_base) return true;
         const bool ok = mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
         ph ^= 1u << s;
         if (ok && tid == 0) sflag[1] &= ~(1 << s);
@@ -669,8 +683,16 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     auto give_up = [&]() {
         if (tid == 0) {
             atomicExch(&P.status->stall, 1);
-            for (int s = 0; s < 3; s++)
+            for (int s = 0; s < 4; s++)
                 if (sflag[1] & (1 << s)) mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
+        }
+    };
+    // the tile's RK base of plane m into the base slot (barrier 3)
+    auto issue_base = [&](int m) {
+        if (S::tma_base && tid == 0) {
+            fence_proxy_async_smem();
+            tma_load_box(sQB, tmb, i0, j0, m, 0, &bar[3], (unsigned)(sizeof(double) * 5 * NT));
+            sflag[1] |= 1 << 3;
         }
     };
 
@@ -768,7 +790,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     auto hflux = [&](int m, int po, int mo, int s, R um, R vm, R wm, R Tm, R up, R vp, R wp_, R Tp, R h[4]) {
         const Slot sl = slot(po);
         const R sc = ktab<R>(P, 0, m);
-        visc_fz<BX>(C, sl, smu(mo)[bc], pres_at(C, sl, spr(mo, s), bc), bc, (up - um) * sc, (vp - vm) * sc,
+        visc_fz<BX>(C, sl, smu(mo)[bc], pres_at<R, S::p_ring>(C, sl, spr(mo, s), bc), bc, (up - um) * sc, (vp - vm) * sc,
                     (wp_ - wm) * sc, (Tp - Tm) * sc, h);
     };
     // hD at the own column of wall plane m, from the wall's own values in
@@ -876,6 +898,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // plane); own column of t+2; (float rings: the own point's RK base
         // starts its way into shared memory); plane t+1's box is converted
         if (t < ke) issue(t + 2, iN);
+        const bool need_base = P.rk_mode != 0;
+        if (S::tma_base && need_base) issue_base(t);
         if (S::prefetch_base) {
             if (P.rk_mode != 0 && out_ok) {
                 const double *src = P.qbase + (long long)t * plane + colo;
@@ -933,17 +957,18 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // ---------- C: viscous flux vectors
         const Slot s0 = slot(pZ), sp = slot(pP);
         R hp1[4] = {0, 0, 0, 0};
+        R fown[4] = {0, 0, 0, 0};   // fD at the own column (exchanged by shuffles when fx_shfl)
         {
             const R czt = ktab<R>(P, 0, t);
             const R *MU = smu(mZ), *PR = spr(mZ, iZ);
             if (col_ok) {
                 if (t + 1 != n3)
                     hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
-                R f[4], g[4];
-                visc_fxy<BX>(C, s0, um1, vm1, wm1, sp, MU, PR, bc, czt, f, g);
+                R g[4];
+                visc_fxy<BX, R, S::p_ring>(C, s0, um1, vm1, wm1, sp, MU, PR, bc, czt, fown, g);
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    sF[(c * TJ + ty) * (TI + 2) + tx + 1] = f[c];
+                    if (!S::fx_shfl) sF[(c * TJ + ty) * (TI + 2) + tx + 1] = fown[c];
                     sG[(c * (TJ + 2) + ty + 1) * TI + tx] = g[c];
                 }
             }
@@ -952,26 +977,46 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 const int ci = side ? i0 + TI : i0 - 1, cj = j0 + r;
                 if (ci <= n1 && cj <= n2) {
                     R f[4];
-                    visc_fx<BX>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR, (r + 2) * BX + (side ? TI + 2 : 1),
-                                czt, f);
+                    visc_fx<BX, R, S::p_ring>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR,
+                                              (r + 2) * BX + (side ? TI + 2 : 1), czt, f);
 #pragma unroll
-                    for (int c = 0; c < 4; c++) sF[c * S::NFX + r * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
+                    for (int c = 0; c < 4; c++) {
+                        if (S::fx_shfl) sF[c * S::NFX + r * 2 + side] = f[c];
+                        else sF[c * S::NFX + r * (TI + 2) + (side ? TI + 1 : 0)] = f[c];
+                    }
                 }
             } else if (hy_lane) {
                 const int h = tid - 32, side = h / TI, cc = h - side * TI;
                 const int ci = i0 + cc, cj = side ? j0 + TJ : j0 - 1;
                 if (ci <= n1 && cj <= n2) {
                     R g[4];
-                    visc_fy<BX>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR, (side ? TJ + 2 : 1) * BX + cc + 2,
-                                czt, g);
+                    visc_fy<BX, R, S::p_ring>(C, s0, sH[tid], sH[S::NHL + tid], sp, MU, PR,
+                                              (side ? TJ + 2 : 1) * BX + cc + 2, czt, g);
 #pragma unroll
                     for (int c = 0; c < 4; c++) sG[c * S::NGY + (side ? TJ + 1 : 0) * TI + cc] = g[c];
                 }
             }
         }
-        __syncthreads();
+        if (S::tma_base && need_base) {
+            bad = !wait_slot(3);
+            if (__syncthreads_or(bad)) { give_up(); return; }
+        } else {
+            __syncthreads();
+        }
 
         // ---------- E: fluxes, source, RK update
+        // fD at the x neighbours: lanes tx+-1 of the row's warp, the halo columns
+        // at the row's ends (every lane takes part in the shuffles)
+        R fxp[4], fxm[4];
+        if (S::fx_shfl) {
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                fxp[c] = __shfl_down_sync(0xffffffffu, fown[c], 1);
+                fxm[c] = __shfl_up_sync(0xffffffffu, fown[c], 1);
+                if (tx == TI - 1) fxp[c] = sF[c * S::NFX + ty * 2 + 1];
+                if (tx == 0) fxm[c] = sF[c * S::NFX + ty * 2 + 0];
+            }
+        }
         R q0[5];
 #pragma unroll
         for (int c = 0; c < 5; c++) q0[c] = sq(iZ, c)[bc];
@@ -1003,8 +1048,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 Fs[0] = F1[0];  // F2 of continuity is zero
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const int r = (c - 1) * TJ + ty;
-                    const R F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * C.hdx;
+                    R F2;
+                    if (S::fx_shfl) {
+                        F2 = (fxp[c - 1] - fxm[c - 1]) * C.hdx;
+                    } else {
+                        const int r = (c - 1) * TJ + ty;
+                        F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * C.hdx;
+                    }
                     Fs[c] = F1[c] + F2;
                 }
             }
@@ -1083,7 +1133,10 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             double qn[5];
             double qb[5] = {0, 0, 0, 0, 0};
             if (P.rk_mode != 0) {
-                if (S::prefetch_base) {
+                if (S::tma_base) {
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qb[c] = sQB[c * NT + tid];
+                } else if (S::prefetch_base) {
                     cp_async_wait<0>();
 #pragma unroll
                     for (int c = 0; c < 5; c++) qb[c] = sQB[c * NT + tid];
@@ -1157,11 +1210,11 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 
 template <int TI, int TJ, typename QI, typename QO, typename R, bool BUOY>
 __global__ void __launch_bounds__(TI *TJ, StageShape<TI, TJ, R>::minb)
-    k_stage(const KParams P, const __grid_constant__ CUtensorMap tmq)
+    k_stage(const KParams P, const __grid_constant__ CUtensorMap tmq, const __grid_constant__ CUtensorMap tmb)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    stage_body<TI, TJ, QI, QO, R, BUOY ? 1 : 0, false>(P, &tmq, blockIdx.x, blockIdx.y, blockIdx.z, threadIdx.x,
-                                                          threadIdx.y, smem_raw);
+    stage_body<TI, TJ, QI, QO, R, BUOY ? 1 : 0, false>(P, &tmq, &tmb, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                          threadIdx.x, threadIdx.y, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -2032,6 +2085,7 @@ struct PPhase {
     unsigned long long need;    // member's completed units before this phase may start
     double dt;                  // clock advance
     const CUtensorMap *tm;      // stage: tensor map of the input buffer
+    const CUtensorMap *tmb;     // stage: tensor map of the RK base (tiles that stage it by bulk copy)
     const double *q;            // statistics: the state buffer
     double *part;               // statistics: partial sums
 };
@@ -2074,7 +2128,7 @@ template <int TI, int TJ, typename QI, typename QO, typename R>
 __device__ __forceinline__ void pstage(const PPhase &F, const KParams &P, int unit, int tid, unsigned char *smem)
 {
     const int bx = unit % F.nx, r = unit / F.nx, by = r % F.ny, bz = r / F.ny;
-    stage_body<TI, TJ, QI, QO, R, 2, true>(P, F.tm, bx, by, bz, tid % TI, tid / TI, smem);
+    stage_body<TI, TJ, QI, QO, R, 2, true>(P, F.tm, F.tmb, bx, by, bz, tid % TI, tid / TI, smem);
 }
 
 #ifndef CHAN_PMINB_MIXED

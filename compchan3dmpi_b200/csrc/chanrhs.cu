@@ -21,7 +21,7 @@ namespace {
 // Stage-kernel tile shapes: TI columns in x (one warp row) by TJ rows in y.
 // Each shape has the plain FP64 kernel and the three mixed-precision stage
 // kernels, without and with the buoyancy term.
-using StageFn = void (*)(const chan::KParams, const CUtensorMap);
+using StageFn = void (*)(const chan::KParams, const CUtensorMap, const CUtensorMap);
 struct StageSet {
     int ti, tj;
     StageFn k[2][4];   // [buoyancy][0 FP64, 1 mixed first stage, 2 mixed middle, 3 mixed last]
@@ -87,6 +87,7 @@ struct chan_ctx {
     // FP64 state buffers, or the two float stage buffers (mixed precision)
     CUtensorMap tmd[CHAN_NTILES][3];
     CUtensorMap tmf[CHAN_NTILES][2];
+    CUtensorMap tmb[CHAN_NTILES];   // the RK base (the FP64 step state) by tile: box TI x TJ x 1 x 5
     int nstage = 2;
     int cur = 0;             // buffer holding the latest state
     bool uploaded = false;
@@ -226,14 +227,14 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 // multiple of TI (16 or 32 elements), so every copy starts on a 16-byte
 // boundary; the rows, planes and variables are px, plane and vol elements
 // apart (multiples of 8 elements).
-int make_state_map(chan_ctx *c, CUtensorMap *m, void *base, bool is_float, int ti, int tj)
+int make_state_map(chan_ctx *c, CUtensorMap *m, void *base, bool is_float, int ti, int tj, int halo = 2)
 {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) { c->err = "cuTensorMapEncodeTiled is not available"; return CHAN_ECUDA; }
     const cuuint64_t es = is_float ? 4 : 8;
     const cuuint64_t dims[4] = {(cuuint64_t)c->n1 + 2, (cuuint64_t)c->n2 + 2, (cuuint64_t)c->n3 + 2, 5};
     const cuuint64_t strides[3] = {(cuuint64_t)c->px * es, (cuuint64_t)c->plane * es, (cuuint64_t)c->vol * es};
-    const cuuint32_t box[4] = {(cuuint32_t)ti + 4, (cuuint32_t)tj + 4, 1, 5};
+    const cuuint32_t box[4] = {(cuuint32_t)(ti + 2 * halo), (cuuint32_t)(tj + 2 * halo), 1, 5};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = enc(m, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base,
                            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -380,8 +381,8 @@ int launch_stage(chan_ctx *c, int iter, bool check, long long step, double time)
         const StageSet &ss = kStageSets[c->tile];
         dim3 grid(c->ntx, c->nty, c->nchunks), block(ss.ti, ss.tj);
         const int v = !c->mixed ? 0 : (iter == 1 ? 1 : (last ? 3 : 2));
-        ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(c->kp,
-                                                                                               stage_map(c));
+        ss.k[c->kp.buoy_on ? 1 : 0][v]<<<grid, block, v == 0 ? ss.smem : ss.smemf, c->stream>>>(
+            c->kp, stage_map(c), c->tmb[c->tile]);
     }
     if (c->closure_on) {
         chan::k_sgs_apply<<<1184, 256, 0, c->stream>>>(c->kp, (double *)c->kp.qout, c->sgsS, c->kp.rk_cdt);
@@ -776,12 +777,15 @@ int chan_init(const chan_params *p, const double *x3, const double *jac, const d
     if (e != cudaSuccess) { fail(nullptr, "cudaFuncSetAttribute", e); chan_free(c); return CHAN_ECUDA; }
     memset(c->tmd, 0, sizeof(c->tmd));
     memset(c->tmf, 0, sizeof(c->tmf));
+    memset(c->tmb, 0, sizeof(c->tmb));
     for (int t = 0; t < CHAN_NTILES; t++) {
         const int ti = kStageSets[t].ti, tj = kStageSets[t].tj;
         for (int b = 0; b < 3 && !c->mixed; b++)
             if ((r = make_state_map(c, &c->tmd[t][b], c->q[b], false, ti, tj))) { g_init_error = c->err; chan_free(c); return r; }
         for (int b = 0; b < 2 && c->mixed; b++)
             if ((r = make_state_map(c, &c->tmf[t][b], c->qf[b], true, ti, tj))) { g_init_error = c->err; chan_free(c); return r; }
+        // the tile's own points (no halo); the x origin 2 + TI*bx gives 16-byte aligned copies
+        if ((r = make_state_map(c, &c->tmb[t], c->q[0], false, ti, tj, 0))) { g_init_error = c->err; chan_free(c); return r; }
     }
     if (set_launch(c, CHAN_TILE_32x8, 0) != CHAN_OK) { g_init_error = c->err; chan_free(c); return CHAN_ECUDA; }
     int sms = 148;
@@ -1685,7 +1689,7 @@ int build_persistent(chan_ensemble *e)
     const size_t n = e->m.size();
     const bool mixed = e->m[0]->mixed;
     std::vector<chan::KParams> kps;
-    std::vector<CUtensorMap> maps;
+    std::vector<CUtensorMap> maps, bmaps;   // per stage record: the input's map; per member: the RK base's
     std::vector<std::vector<chan::PPhase>> per(n);
     for (size_t i = 0; i < n; i++) {
         chan_ctx *c = e->m[i];
@@ -1698,6 +1702,7 @@ int build_persistent(chan_ensemble *e)
             kps.push_back(k);
             maps.push_back(stage_map(c));
         }
+        bmaps.push_back(c->tmb[c->tile]);
         unsigned long long need = 0;
         auto add = [&](chan::PPhase ph) {
             ph.member = (int)i;
@@ -1755,9 +1760,14 @@ int build_persistent(chan_ensemble *e)
         for (size_t i = 0; i < n; i++)
             if (q < per[i].size())
                 for (int u = 0; u < per[i][q].units; u++) items.push_back({(int)(first[i] + q), u});
+    const size_t nmaps = maps.size();
+    maps.insert(maps.end(), bmaps.begin(), bmaps.end());
     EK(e, ensure_dev(&e->dmaps, &e->cap_maps, maps.size()));
     for (auto &f : ph)
-        if (f.kind == chan::kPStage) f.tm = e->dmaps + f.kp;
+        if (f.kind == chan::kPStage) {
+            f.tm = e->dmaps + f.kp;
+            f.tmb = e->dmaps + nmaps + f.member;
+        }
     if (e->stall_test && !ph.empty()) {
         // host-side fault injection: member 0's first stage waits for a unit count never reached
         for (size_t k = 0; k < per[0].size(); k++)
