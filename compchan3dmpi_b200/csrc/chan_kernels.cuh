@@ -908,12 +908,22 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
             cp_async_commit();
         }
-#ifdef CHAN_PREFETCH_BASE_L1
-        // the own point's RK base into L1 now; the update reads it at the end of the plane
-        if (!S::prefetch_base && P.rk_mode != 0 && out_ok) {
+#ifndef CHAN_NO_PREFETCH_BASE_L1
+        // the own point's RK base into L1 now; the update reads it at the end of
+        // the plane (2.7% of the FP64 stage time against loading it there cold)
+        if (!S::prefetch_base && !S::tma_base && P.rk_mode != 0 && out_ok) {
             const double *src = P.qbase + (long long)t * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+        }
+#endif
+#ifdef CHAN_PREFETCH_TABLES
+        // next plane's per-plane coefficients and forcing density into L1 (one
+        // lane each; every thread of the CTA reads them at the next plane)
+        if (t < ke && tid < 6) {
+            const double *a = tid == 0 ? P.czh : (tid == 1 ? P.cz8 : (tid == 2 ? P.cz12 : (tid == 3 ? P.pez : P.stat)));
+            const int k = tid == 4 ? t : (tid == 5 ? t + 2 : t + 1);
+            if (tid != 5 || t + 2 <= n3) asm volatile("prefetch.global.L1 [%0];" ::"l"(tid == 5 ? P.czh + k : a + k));
         }
 #endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
