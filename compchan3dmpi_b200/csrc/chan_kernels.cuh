@@ -917,15 +917,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
 #endif
-#ifdef CHAN_PREFETCH_TABLES
-        // next plane's per-plane coefficients and forcing density into L1 (one
-        // lane each; every thread of the CTA reads them at the next plane)
-        if (t < ke && tid < 6) {
-            const double *a = tid == 0 ? P.czh : (tid == 1 ? P.cz8 : (tid == 2 ? P.cz12 : (tid == 3 ? P.pez : P.stat)));
-            const int k = tid == 4 ? t : (tid == 5 ? t + 2 : t + 1);
-            if (tid != 5 || t + 2 <= n3) asm volatile("prefetch.global.L1 [%0];" ::"l"(tid == 5 ? P.czh + k : a + k));
-        }
-#endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
 #ifdef CHAN_LATE_CENTER
         // own column of plane t+2: loads issued now, primitives formed after the
