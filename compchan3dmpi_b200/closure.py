@@ -300,6 +300,33 @@ def _errors(les, dns):
             "uw_peak": abs(pk(les["uw"]) - pk(dns["uw"])) / pk(dns["uw"])}
 
 
+def _seeds(s):
+    """A seed or a sequence of seeds, as a tuple."""
+    return tuple(int(x) for x in s) if isinstance(s, (tuple, list)) else (int(s),)
+
+
+def mean_stats(stats):
+    """The statistics of several coarse runs averaged run by run: Cf, Re_tau and
+    u_tau, and each profile point by point (the same grid for every run)."""
+    out = {}
+    for k in stats[0]:
+        v = [st[k] for st in stats]
+        out[k] = np.mean(np.asarray(v, dtype=np.float64), axis=0).tolist() if isinstance(v[0], list) \
+            else float(np.mean(v))
+    return out
+
+
+def seed_runs(runs):
+    """Coarse runs from several seeds as one result: the statistics averaged
+    over the runs (None if any run blew up or fell back), the first fallback
+    report, the mean wall time of a run, and the runs themselves."""
+    ok = all(r["stats"] is not None and r["report"]["fallback_step"] is None for r in runs)
+    rep = next((r["report"] for r in runs if r["report"]["fallback_step"] is not None or r["report"]["reason"]),
+               runs[0]["report"])
+    return {"steps": runs[0]["steps"], "wall_s": float(np.mean([r["wall_s"] for r in runs])), "report": rep,
+            "stats": mean_stats([r["stats"] for r in runs]) if ok else None, "per_seed": runs}
+
+
 def wall_shear_history(ch: Channel, steps: int, every: int):
     """Step ``steps`` steps in chunks of ``every`` (a multiple of istat) and
     record (time, wall shear (tauL - tauU)/2) after each chunk."""
@@ -403,7 +430,8 @@ def _train_and_calibrate(name, sources, deficit, pcc, x3c, jacc, invc, start, ca
     """One training set: the samples of ``sources`` (closure datasets with their
     snapshot layout) with the coarse solver's shear-stress deficit added to
     tau_uw; training; the magnitude alpha picked by coarse runs from the
-    calibration seed.  Returns (closure, normalisation, alpha, report)."""
+    calibration seeds (their statistics averaged over the runs).  Returns
+    (closure, normalisation, alpha, report)."""
     cl = Closure(capacity=sum(src.count for src, _, _ in sources))
     for src, per_snap, per_plane in sources:
         add_shear_deficit(src, cl, deficit, per_snap, per_plane)
@@ -418,9 +446,14 @@ def _train_and_calibrate(name, sources, deficit, pcc, x3c, jacc, invc, start, ca
     cal = {}
     for a in alphas:
         cl.norm = scaled_norm(norm0, a)
-        r = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, cl)
-        e = _errors(r["stats"], dns_c) if r["stats"] and r["report"]["fallback_step"] is None else None
-        cal[a] = {"report": r["report"], "errors": e, "wall_s": r["wall_s"]}
+        runs = []
+        for sd in _seeds(cal_seed):
+            runs.append(coarse_run(pcc, x3c, jacc, invc, start(sd), coarse_steps, cl))
+            if runs[-1]["report"]["fallback_step"] is not None or runs[-1]["stats"] is None:
+                break   # this alpha is out: the other seeds need not run
+        r = seed_runs(runs)
+        e = _errors(r["stats"], dns_c) if r["stats"] else None
+        cal[a] = {"report": r["report"], "errors": e, "wall_s": r["wall_s"], "seeds_run": len(runs)}
         log(json.dumps({"phase": f"calibration ({name})", "alpha": a, **cal[a]}))
     ok = {a: c for a, c in cal.items() if c["errors"] is not None}
     best = min(ok, key=lambda a: ok[a]["errors"]["Cf"] + ok[a]["errors"]["uw_peak"]) if ok else None
@@ -441,19 +474,22 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
        width-``filter_width`` filtered DNS is sampled into the dataset and the
        statistics are time-averaged; the wall shear is recorded every
        ``rec_every`` steps to show whether the window is stationary.
-    2. A plain coarse run (``coarse_steps`` steps from a seeded smooth
-       perturbation, statistics over its second half) gives what the coarse
-       solver misses: the deficit of its mean Reynolds shear stress rho<u'w'>
-       against the DNS at its wall-normal points.  ``coarse_snapshots`` of its
+    2. Plain coarse runs (``coarse_steps`` steps from seeded smooth
+       perturbations, one per calibration seed, statistics over each run's
+       second half, averaged over the runs) give what the coarse solver
+       misses: the deficit of its mean Reynolds shear stress rho<u'w'> against
+       the DNS at its wall-normal points.  ``coarse_snapshots`` of each run's
        own closure inputs are sampled over the same half.
     3. Two training sets, each with that deficit added to tau_uw plane by
        plane: the filtered-DNS samples with their subgrid fluxes, and those plus
        the coarse run's own inputs (deficit targets only), which are the inputs
        the closure meets in a coarse run.
     4. For each, the closure's magnitude alpha (its outputs scaled by alpha) is
-       chosen by coarse runs from a calibration seed; the better training set
-       by that score is then compared, plain against closure, in coarse runs
-       from another seed.
+       chosen by coarse runs from the calibration seeds; the better training
+       set by that score is then compared, plain against closure, in coarse
+       runs from the evaluation seeds (statistics averaged over the runs, and
+       each run's own errors).  ``cal_seed`` and ``eval_seed`` are a seed or a
+       sequence of seeds.
     """
     t_all = time.time()
     kst = (dns_grid[2] - 1) // (coarse_grid[2] - 1)
@@ -503,15 +539,16 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
     # coarse starts and dt: seeded smooth perturbations on the coarse grid
     def start(sd):
         return smooth_start(pc, x3c, seed=sd)
-    dtc = cfl_dt(start(cal_seed), pc, jacc, cfl)
+    cal_seeds, eval_seeds = _seeds(cal_seed), _seeds(eval_seed)
+    dtc = cfl_dt(start(cal_seeds[0]), pc, jacc, cfl)
     pcc = pc.with_(dt=dtc)
     c1, c2, c3 = coarse_grid
     cper_plane, cper_snap = (c1 - 2) * (c2 - 2), (c1 - 2) * (c2 - 2) * (c3 - 2)
-    craw = Closure(capacity=(coarse_snapshots + 1) * cper_snap)
+    craw = Closure(capacity=(coarse_snapshots + 1) * cper_snap * len(cal_seeds))
     every = max(((coarse_steps - coarse_steps // 2) // max(coarse_snapshots, 1)) // pcc.istat, 1) * pcc.istat
-    plain_cal = coarse_run(pcc, x3c, jacc, invc, start(cal_seed), coarse_steps, sample_into=craw,
-                           sample_every=every)
-    log(json.dumps({"phase": "coarse plain (calibration seed)", "wall_s": plain_cal["wall_s"],
+    plain_cal = seed_runs([coarse_run(pcc, x3c, jacc, invc, start(sd), coarse_steps, sample_into=craw,
+                                      sample_every=every) for sd in cal_seeds])
+    log(json.dumps({"phase": "coarse plain (calibration seeds)", "wall_s": plain_cal["wall_s"],
                     "samples": craw.count,
                     "errors": _errors(plain_cal["stats"], dns_c) if plain_cal["stats"] else None}))
     if plain_cal["stats"] is None:
@@ -529,16 +566,19 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
                                              coarse_steps, dns_c, epochs, batch, lr, seed, alphas, log)
     ok = {n: t for n, t in trained.items() if t[2] is not None}
     chosen = min(ok, key=lambda n: ok[n][3]["score"]) if ok else None
-    # evaluation from another seed: plain against the calibrated closure
-    runs = {"plain": coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps)}
+    # evaluation from other seeds: plain against the calibrated closure
+    runs = {"plain": seed_runs([coarse_run(pcc, x3c, jacc, invc, start(sd), coarse_steps) for sd in eval_seeds])}
     if chosen is not None:
         cl, norm0, best, _ = trained[chosen]
         cl.norm = scaled_norm(norm0, best)
-        runs["closure"] = coarse_run(pcc, x3c, jacc, invc, start(eval_seed), coarse_steps, cl)
+        runs["closure"] = seed_runs([coarse_run(pcc, x3c, jacc, invc, start(sd), coarse_steps, cl)
+                                     for sd in eval_seeds])
     for name, r in runs.items():
         r["errors_vs_dns"] = _errors(r["stats"], dns_c) if r["stats"] else None
-        log(json.dumps({"phase": f"coarse {name} (evaluation seed)", "wall_s": r["wall_s"], "report": r["report"],
-                        "errors": r["errors_vs_dns"]}))
+        for q in r["per_seed"]:
+            q["errors_vs_dns"] = _errors(q["stats"], dns_c) if q["stats"] else None
+        log(json.dumps({"phase": f"coarse {name} (evaluation seeds)", "wall_s": r["wall_s"], "report": r["report"],
+                        "errors": r["errors_vs_dns"], "per_seed": [q["errors_vs_dns"] for q in r["per_seed"]]}))
     fp64_window_s = fp64_ms * 1e-3 * snapshots * snap_every
     fp64_coarse_equiv_s = fp64_ms * 1e-3 * (coarse_steps * pcc.dt / pd.dt)
     out = {"dns": {"nP": list(dns_grid), "Re": pd.Re, "dt": pd.dt, "spinup_steps": spinup,
@@ -547,7 +587,7 @@ def experiment(dns_grid=(256, 192, 193), coarse_grid=(64, 64, 65), spinup=150000
                    "stationarity_spinup_last_half": stationarity(hist_spin[len(hist_spin) // 2:]),
                    "fp64_ms_per_step": fp64_ms, "fp64_window_s": fp64_window_s},
            "coarse": {"nP": list(coarse_grid), "dt": pcc.dt, "steps": coarse_steps,
-                      "seeds": {"calibration": cal_seed, "evaluation": eval_seed},
+                      "seeds": {"calibration": list(cal_seeds), "evaluation": list(eval_seeds)},
                       "deficit_rho_uw": deficit.tolist(), "training_sets": {n: t[3] for n, t in trained.items()},
                       "chosen": chosen, "alpha": trained[chosen][2] if chosen else None, "runs": runs},
            "wall_time_fp64_dns_same_physical_time_over_closure":
@@ -605,6 +645,10 @@ def main(argv=None):
     ap.add_argument("--re", type=float, default=None, help="Reynolds number (default: the production 3000)")
     ap.add_argument("--coarse-snapshots", type=int, default=50)
     ap.add_argument("--rec-every", type=int, default=1000)
+    ap.add_argument("--cal-seeds", type=int, nargs="+", default=[21, 27, 29],
+                    help="seeds of the coarse runs that give the deficit and pick alpha")
+    ap.add_argument("--eval-seeds", type=int, nargs="+", default=[33, 41, 47],
+                    help="seeds of the held-out coarse runs, plain against closure")
     ap.add_argument("--out", default=None, help="write the JSON report here")
     ap.add_argument("--weights", default=None, help="save the trained closure (npz) here")
     a = ap.parse_args(argv)
@@ -614,7 +658,8 @@ def main(argv=None):
     res, params, norm = experiment(tuple(a.dns_grid), tuple(a.coarse_grid), a.spinup, a.snapshots, a.snap_every,
                                    a.coarse_steps, a.epochs, a.batch, a.lr, cfl=a.cfl, alphas=tuple(a.alphas),
                                    filter_width=a.filter_width, rec_every=a.rec_every,
-                                   coarse_snapshots=a.coarse_snapshots, Re=a.re, log=lambda s: print(s, flush=True))
+                                   coarse_snapshots=a.coarse_snapshots, Re=a.re, cal_seed=tuple(a.cal_seeds),
+                                   eval_seed=tuple(a.eval_seeds), log=lambda s: print(s, flush=True))
     if a.weights and params is not None:
         np.savez(a.weights, params=params, norm=norm)
     s = json.dumps(res)

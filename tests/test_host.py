@@ -308,3 +308,21 @@ def test_closure_deficit_targets_and_magnitude_knob():
     flat = stationarity([(t, 1.0) for t in range(10)])
     rising = stationarity([(t, 1.0 + 0.1 * t) for t in range(10)])
     assert abs(flat["drift"]) < 1e-12 and rising["drift"] > 0.3 and rising["halves"] > 0.2
+
+
+def test_closure_runs_over_several_seeds_combine():
+    """Coarse runs from several seeds: statistics averaged run by run, profiles
+    point by point; a run that fell back or blew up leaves no statistics and
+    its report is the one kept."""
+    from compchan3dmpi_b200.closure import mean_stats, seed_runs
+    ok = {"fallback_step": None, "reason": None, "plain_failed": None}
+    a = {"steps": 10, "wall_s": 1.0, "report": ok, "stats": {"Cf": 1.0, "uw": [0.0, 2.0]}}
+    b = {"steps": 10, "wall_s": 3.0, "report": ok, "stats": {"Cf": 2.0, "uw": [1.0, 4.0]}}
+    m = mean_stats([a["stats"], b["stats"]])
+    assert m == {"Cf": 1.5, "uw": [0.5, 3.0]}
+    r = seed_runs([a, b])
+    assert r["stats"] == m and r["wall_s"] == 2.0 and r["report"] == ok and len(r["per_seed"]) == 2
+    fell = {"steps": 10, "wall_s": 2.0, "stats": {"Cf": 9.0, "uw": [9.0, 9.0]},
+            "report": {"fallback_step": 400, "reason": "closure output beyond its limit", "plain_failed": None}}
+    r = seed_runs([a, fell])
+    assert r["stats"] is None and r["report"]["fallback_step"] == 400
