@@ -1166,14 +1166,35 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             const int im = (i <= 3) ? i + (n1 - 2) : ((i >= n1 - 2) ? i - (n1 - 2) : -1);
             const int jm = (j <= 3) ? j + (n2 - 2) : ((j >= n2 - 2) ? j - (n2 - 2) : -1);
             const long long pk = (long long)t * plane;
+#ifdef CHAN_IMAGE_BRANCH
+            constexpr bool img_branch = sizeof(R) == 8;
+#else
+            constexpr bool img_branch = false;
+#endif
+            if (img_branch) {
+                // own point; then, only at points within 2 of a periodic edge, the images
 #pragma unroll
-            for (int c = 0; c < 5; c++) {
-                QO *O = qout() + c * vol + pk;
-                const QO v = (QO)qn[c];
-                O[(long long)j * P.px + i] = v;
-                if (im >= 0) O[(long long)j * P.px + im] = v;
-                if (jm >= 0) O[(long long)jm * P.px + i] = v;
-                if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = v;
+                for (int c = 0; c < 5; c++) qout()[c * vol + pk + colo] = (QO)qn[c];
+                if (im >= 0 || jm >= 0) {
+#pragma unroll
+                    for (int c = 0; c < 5; c++) {
+                        QO *O = qout() + c * vol + pk;
+                        const QO v = (QO)qn[c];
+                        if (im >= 0) O[(long long)j * P.px + im] = v;
+                        if (jm >= 0) O[(long long)jm * P.px + i] = v;
+                        if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = v;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 5; c++) {
+                    QO *O = qout() + c * vol + pk;
+                    const QO v = (QO)qn[c];
+                    O[(long long)j * P.px + i] = v;
+                    if (im >= 0) O[(long long)j * P.px + im] = v;
+                    if (jm >= 0) O[(long long)jm * P.px + i] = v;
+                    if (im >= 0 && jm >= 0) O[(long long)jm * P.px + im] = v;
+                }
             }
             if (P.check) {
                 const double tr = qn[0] * qn[4] - P.ggMh * ((qn[1] * qn[1] + qn[2] * qn[2]) + qn[3] * qn[3]);
