@@ -1166,7 +1166,10 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             const int im = (i <= 3) ? i + (n1 - 2) : ((i >= n1 - 2) ? i - (n1 - 2) : -1);
             const int jm = (j <= 3) ? j + (n2 - 2) : ((j >= n2 - 2) ? j - (n2 - 2) : -1);
             const long long pk = (long long)t * plane;
-#ifdef CHAN_IMAGE_BRANCH
+            // FP64 rings: the periodic images under one branch that only points within 2
+            // of a periodic edge take (0.7% of the stage time); the float rings keep
+            // predicated stores (the branch costs them spills)
+#ifndef CHAN_NO_IMAGE_BRANCH
             constexpr bool img_branch = sizeof(R) == 8;
 #else
             constexpr bool img_branch = false;
