@@ -153,46 +153,54 @@ __device__ __forceinline__ void flag_nonfinite(DevStatus *st, int i, int j, int 
 //  QUICK   : ue*Qe - uw*Qw, face values upwinded on the face velocity sign,
 //            the four sign branches of main_v1.9.f90:335-361
 template <typename R>
+__device__ __forceinline__ void quick_weights(R um1, R u0, R up1, R s8, R w[5])
+{
+    const R r1 = (u0 + up1) * R(0.5);  // tmpR1, east face
+    const R r2 = (u0 + um1) * R(0.5);  // tmpR2, west face
+    const bool e = r1 >= R(0), f = r2 >= R(0);
+    const R R1 = r1 * s8, R2 = r2 * s8;
+    // east face value at offsets -1,0,+1,+2 ; west face at -2,-1,0,+1
+    const R ae_m1 = e ? R(-1) : R(0), ae_0 = e ? R(6) : R(3), ae_1 = e ? R(3) : R(6), ae_2 = e ? R(0) : R(-1);
+    const R bw_m2 = f ? R(-1) : R(0), bw_m1 = f ? R(6) : R(3), bw_0 = f ? R(3) : R(6), bw_1 = f ? R(0) : R(-1);
+    w[0] = -R2 * bw_m2;
+    w[1] = R1 * ae_m1 - R2 * bw_m1;
+    w[2] = R1 * ae_0 - R2 * bw_0;
+    w[3] = R1 * ae_1 - R2 * bw_1;
+    w[4] = R1 * ae_2;
+}
+
+template <typename R>
+__device__ __forceinline__ void central_weights(R um2, R um1, R up1, R up2, R s12, R w[5])
+{
+    w[0] = um2 * s12;
+    w[1] = R(-8) * um1 * s12;
+    w[2] = R(0);
+    w[3] = R(8) * up1 * s12;
+    w[4] = -(up2 * s12);
+}
+
+template <typename R>
 __device__ __forceinline__ void inv_weights(R um2, R um1, R u0, R up1, R up2, bool quick, R s8, R s12, R w[5])
 {
-#ifdef CHAN_INV_SELECT
-    if (sizeof(R) == 8) {
-        // both weight sets, then a select per weight: no branch for lanes that disagree
-        const R r1 = (u0 + up1) * R(0.5), r2 = (u0 + um1) * R(0.5);
-        const bool e = r1 >= R(0), f = r2 >= R(0);
-        const R R1 = r1 * s8, R2 = r2 * s8;
-        const R ae_m1 = e ? R(-1) : R(0), ae_0 = e ? R(6) : R(3), ae_1 = e ? R(3) : R(6), ae_2 = e ? R(0) : R(-1);
-        const R bw_m2 = f ? R(-1) : R(0), bw_m1 = f ? R(6) : R(3), bw_0 = f ? R(3) : R(6), bw_1 = f ? R(0) : R(-1);
-        const R q0 = -R2 * bw_m2, q1 = R1 * ae_m1 - R2 * bw_m1, q2 = R1 * ae_0 - R2 * bw_0;
-        const R q3 = R1 * ae_1 - R2 * bw_1, q4 = R1 * ae_2;
-        const R c0 = um2 * s12, c1 = R(-8) * um1 * s12, c3 = R(8) * up1 * s12, c4 = -(up2 * s12);
-        w[0] = quick ? q0 : c0;
-        w[1] = quick ? q1 : c1;
-        w[2] = quick ? q2 : R(0);
-        w[3] = quick ? q3 : c3;
-        w[4] = quick ? q4 : c4;
-        return;
-    }
+    // FP64: both weight sets, then a select per weight.  The switch differs from
+    // lane to lane where the cell Peclet number crosses its limit, and a branch
+    // there runs both paths one after the other (2.6% of the FP64 stage time).
+    // The float kernels keep the branch.
+#ifdef CHAN_INV_SELECT_F
+    constexpr bool sel = true;
+#else
+    constexpr bool sel = sizeof(R) == 8;
 #endif
-    if (quick) {
-        const R r1 = (u0 + up1) * R(0.5);  // tmpR1, east face
-        const R r2 = (u0 + um1) * R(0.5);  // tmpR2, west face
-        const bool e = r1 >= R(0), f = r2 >= R(0);
-        const R R1 = r1 * s8, R2 = r2 * s8;
-        // east face value at offsets -1,0,+1,+2 ; west face at -2,-1,0,+1
-        const R ae_m1 = e ? R(-1) : R(0), ae_0 = e ? R(6) : R(3), ae_1 = e ? R(3) : R(6), ae_2 = e ? R(0) : R(-1);
-        const R bw_m2 = f ? R(-1) : R(0), bw_m1 = f ? R(6) : R(3), bw_0 = f ? R(3) : R(6), bw_1 = f ? R(0) : R(-1);
-        w[0] = -R2 * bw_m2;
-        w[1] = R1 * ae_m1 - R2 * bw_m1;
-        w[2] = R1 * ae_0 - R2 * bw_0;
-        w[3] = R1 * ae_1 - R2 * bw_1;
-        w[4] = R1 * ae_2;
+    if (sel) {
+        R a[5], b[5];
+        quick_weights(um1, u0, up1, s8, a);
+        central_weights(um2, um1, up1, up2, s12, b);
+#pragma unroll
+        for (int m = 0; m < 5; m++) w[m] = quick ? a[m] : b[m];
+    } else if (quick) {
+        quick_weights(um1, u0, up1, s8, w);
     } else {
-        w[0] = um2 * s12;
-        w[1] = R(-8) * um1 * s12;
-        w[2] = R(0);
-        w[3] = R(8) * up1 * s12;
-        w[4] = -(up2 * s12);
+        central_weights(um2, um1, up1, up2, s12, w);
     }
 }
 
@@ -1112,21 +1120,22 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 const R czt = ktab<R>(P, 0, t);
                 Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
-#ifdef CHAN_TOP_HOIST
-                // (hp1 is not formed on the top plane, and the march ends there)
-                if (top) {
+                // FP64 rings: the top plane's hD from the prologue's staging, under one
+                // uniform branch (hp1 is not formed on the top plane, and the march ends
+                // there); 1% of the FP64 stage time
+#ifdef CHAN_TOP_HOIST_F
+                constexpr bool hoist = true;
+#else
+                constexpr bool hoist = sizeof(R) == 8;
+#endif
+                if (hoist && top) {
 #pragma unroll
                     for (int c = 0; c < 4; c++) hp1[c] = (R)P.hwt[c * plane + colo];
                 }
-#endif
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
                     const R H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(iP, c)[bc], qp2[c]);
-#ifdef CHAN_TOP_HOIST
-                    const R hp = hp1[c - 1];
-#else
-                    const R hp = top ? (R)P.hwt[(c - 1) * plane + colo] : hp1[c - 1];
-#endif
+                    const R hp = hoist ? hp1[c - 1] : (top ? (R)P.hwt[(c - 1) * plane + colo] : hp1[c - 1]);
                     const R H2 = (hp - hm1[c - 1]) * czt;
                     Fs[c] = (Fs[c] + H1) + H2;
                 }
