@@ -182,14 +182,14 @@ __device__ __forceinline__ void central_weights(R um2, R um1, R up1, R up2, R s1
 template <typename R>
 __device__ __forceinline__ void inv_weights(R um2, R um1, R u0, R up1, R up2, bool quick, R s8, R s12, R w[5])
 {
-    // FP64: both weight sets, then a select per weight.  The switch differs from
-    // lane to lane where the cell Peclet number crosses its limit, and a branch
-    // there runs both paths one after the other (2.6% of the FP64 stage time).
-    // The float kernels keep the branch.
-#ifdef CHAN_INV_SELECT_F
+    // Both weight sets, then a select per weight.  The switch differs from lane
+    // to lane where the cell Peclet number crosses its limit, and a branch there
+    // runs both paths one after the other (2.6% of the FP64 stage time, 1% of the
+    // float one together with the top-plane hoist below).
+#ifndef CHAN_INV_BRANCH
     constexpr bool sel = true;
 #else
-    constexpr bool sel = sizeof(R) == 8;
+    constexpr bool sel = false;
 #endif
     if (sel) {
         R a[5], b[5];
@@ -385,9 +385,34 @@ __device__ __forceinline__ int wrap_idx(int i, int n)
 // rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from a
 // float seed (relative error 2^-23 -> ~1e-14 -> ~1 ulp).  Valid for |x| in
 // the float normal range, which covers rho and mu of any physical state.
+// The float seeds: with CHAN_FAST_SEEDS the hardware approximations themselves
+// (rcp.approx, ex2.approx; relative errors about 2^-23 and 2^-22), which the
+// FP64 refinement takes to the same accuracy; otherwise the correctly rounded
+// float reciprocal and the float exp2.
+__device__ __forceinline__ float seed_rcp(float x)
+{
+#ifdef CHAN_FAST_SEEDS
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return __frcp_rn(x);
+#endif
+}
+__device__ __forceinline__ float seed_exp2(float x)
+{
+#ifdef CHAN_FAST_SEEDS
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return exp2f(x);
+#endif
+}
+
 __device__ __forceinline__ double rcp_fast(double x)
 {
-    double r = (double)__frcp_rn((float)x);
+    double r = (double)seed_rcp((float)x);
     double e = fma(-x, r, 1.0);
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
@@ -402,7 +427,7 @@ __device__ __forceinline__ double rcp_fast(double x)
 __device__ __forceinline__ double pow07(double T)
 {
     const float tf = (float)T;
-    double y = (double)exp2f(0.7f * __log2f(tf));
+    double y = (double)seed_exp2(0.7f * __log2f(tf));
     const double T2 = T * T, T4 = T2 * T2, a = (T4 * T2) * T;
     const double y2 = y * y, y4 = y2 * y2, y8 = y4 * y4, u = y8 * y2;
     const double num = fma(9.0, u, 11.0 * a);
@@ -1120,13 +1145,15 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 const R czt = ktab<R>(P, 0, t);
                 Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
-                // FP64 rings: the top plane's hD from the prologue's staging, under one
+                // float rings: the top plane's hD from the prologue's staging, under one
                 // uniform branch (hp1 is not formed on the top plane, and the march ends
-                // there); 1% of the FP64 stage time
-#ifdef CHAN_TOP_HOIST_F
+                // there).  Measured with the select weights: 1% faster in the float
+                // kernels, 1% slower in the FP64 one (register allocation), which keeps
+                // the select inside the flux loop.
+#ifdef CHAN_TOP_HOIST_D
                 constexpr bool hoist = true;
 #else
-                constexpr bool hoist = sizeof(R) == 8;
+                constexpr bool hoist = sizeof(R) == 4;
 #endif
                 if (hoist && top) {
 #pragma unroll
