@@ -385,13 +385,14 @@ __device__ __forceinline__ int wrap_idx(int i, int n)
 // rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from a
 // float seed (relative error 2^-23 -> ~1e-14 -> ~1 ulp).  Valid for |x| in
 // the float normal range, which covers rho and mu of any physical state.
-// The float seeds: with CHAN_FAST_SEEDS the hardware approximations themselves
-// (rcp.approx, ex2.approx; relative errors about 2^-23 and 2^-22), which the
-// FP64 refinement takes to the same accuracy; otherwise the correctly rounded
-// float reciprocal and the float exp2.
+// The float seeds are the hardware approximations themselves (rcp.approx,
+// ex2.approx; relative errors about 2^-23 and 2^-22), which the FP64
+// refinement takes to the same accuracy.  Seeding from the correctly rounded
+// float reciprocal and the float library exp2 instead (CHAN_EXACT_SEEDS) made
+// the FP64 stage kernel 7.5% slower and the float one 2.7%.
 __device__ __forceinline__ float seed_rcp(float x)
 {
-#ifdef CHAN_FAST_SEEDS
+#ifndef CHAN_EXACT_SEEDS
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
@@ -401,7 +402,7 @@ __device__ __forceinline__ float seed_rcp(float x)
 }
 __device__ __forceinline__ float seed_exp2(float x)
 {
-#ifdef CHAN_FAST_SEEDS
+#ifndef CHAN_EXACT_SEEDS
     float r;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
@@ -557,7 +558,17 @@ __device__ __forceinline__ R mu_of(double T);
 template <>
 __device__ __forceinline__ double mu_of<double>(double T) { return pow07(T); }
 template <>
-__device__ __forceinline__ float mu_of<float>(double T) { return exp2f(0.7f * log2f((float)T)); }
+__device__ __forceinline__ float mu_of<float>(double T)
+{
+#ifdef CHAN_FAST_MU_F
+    // the hardware log2 and exp2 approximations (relative error about 2^-21)
+    float l;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"((float)T));
+    return seed_exp2(0.7f * l);
+#else
+    return exp2f(0.7f * log2f((float)T));
+#endif
+}
 
 // a load of state written earlier in the same launch by other CTAs (the
 // persistent ensemble kernel) must not use the read-only path
@@ -1326,10 +1337,18 @@ __device__ __forceinline__ void inner_uvT(const KParams &P, int i, int j, int k,
     }
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
     const double q0 = qo[o];
+#ifdef CHAN_FAST_DIV
+    const double r = rcp_fast(q0);
+    u = (double)qo[P.vol + o] * r;
+    v = (double)qo[2 * P.vol + o] * r;
+    const double w = (double)qo[3 * P.vol + o] * r;
+    const double E = (double)qo[4 * P.vol + o] * r;
+#else
     u = (double)qo[P.vol + o] / q0;
     v = (double)qo[2 * P.vol + o] / q0;
     const double w = (double)qo[3 * P.vol + o] / q0;
     const double E = (double)qo[4 * P.vol + o] / q0;
+#endif
     T = E - P.ggMh * ((u * u + v * v) + w * w);
 }
 
@@ -1393,14 +1412,24 @@ __device__ __forceinline__ void wall_body(const KParams &P, int bx_, int by_, in
             const long long o = (long long)(pl == 0 ? k2 : k3) * plane + (long long)jj * P.px + ii;
             const double q0 = qo[o], q1 = qo[vol + o], q2 = qo[2 * vol + o];
             const double q3 = qo[3 * vol + o], q4 = qo[4 * vol + o];
+#ifdef CHAN_FAST_DIV
+            const double r = rcp_fast(q0);
+            const double u = q1 * r, v = q2 * r, w = q3 * r;
+            const double E = q4 * r;
+#else
             const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
             const double E = q4 / q0;
+#endif
             const double T = E - P.ggMh * ((u * u + v * v) + w * w);
             sp[pl][0][by][bx] = q0;
             sp[pl][1][by][bx] = u;
             sp[pl][2][by][bx] = v;
             sp[pl][3][by][bx] = w;
+#ifdef CHAN_FAST_DIV
+            sp[pl][4][by][bx] = (q0 * T) * P.inv_gM2;
+#else
             sp[pl][4][by][bx] = (q0 * T) / P.gM2;
+#endif
             sp[pl][5][by][bx] = pow07(T);
         }
     }
@@ -1519,12 +1548,23 @@ __device__ __forceinline__ void ref_var(const KParams &P, const double *q, int i
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
     const double q0 = q[o];
     x[0] = q0;
+#ifdef CHAN_FAST_DIV
+    // one reciprocal for the four quotients (within an ulp or two of them)
+    const double r = rcp_fast(q0);
+    x[1] = q[P.vol + o] * r;
+    x[2] = q[2 * P.vol + o] * r;
+    x[3] = q[3 * P.vol + o] * r;
+    x[4] = q[4 * P.vol + o] * r;
+    x[5] = x[4] - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
+    x[6] = (x[0] * x[5]) * P.inv_gM2;
+#else
     x[1] = q[P.vol + o] / q0;
     x[2] = q[2 * P.vol + o] / q0;
     x[3] = q[3 * P.vol + o] / q0;
     x[4] = q[4 * P.vol + o] / q0;
     x[5] = x[4] - P.ggMh * ((x[1] * x[1] + x[2] * x[2]) + x[3] * x[3]);
     x[6] = (x[0] * x[5]) / P.gM2;
+#endif
 }
 
 // Plane moments (avgSpatial, main_v1.9.f90:995-1025) and wall shear
