@@ -560,8 +560,10 @@ __device__ __forceinline__ double mu_of<double>(double T) { return pow07(T); }
 template <>
 __device__ __forceinline__ float mu_of<float>(double T)
 {
-#ifdef CHAN_FAST_MU_F
-    // the hardware log2 and exp2 approximations (relative error about 2^-21)
+    // the hardware log2 and exp2 approximations (relative error about 2^-21, well
+    // inside the float path's own rounding); the library log2f/exp2f cost 2.5% of
+    // the float stage kernel (CHAN_LIBM_MU_F)
+#ifndef CHAN_LIBM_MU_F
     float l;
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"((float)T));
     return seed_exp2(0.7f * l);
@@ -1337,7 +1339,7 @@ __device__ __forceinline__ void inner_uvT(const KParams &P, int i, int j, int k,
     }
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
     const double q0 = qo[o];
-#ifdef CHAN_FAST_DIV
+#ifndef CHAN_TRUE_DIV
     const double r = rcp_fast(q0);
     u = (double)qo[P.vol + o] * r;
     v = (double)qo[2 * P.vol + o] * r;
@@ -1412,7 +1414,7 @@ __device__ __forceinline__ void wall_body(const KParams &P, int bx_, int by_, in
             const long long o = (long long)(pl == 0 ? k2 : k3) * plane + (long long)jj * P.px + ii;
             const double q0 = qo[o], q1 = qo[vol + o], q2 = qo[2 * vol + o];
             const double q3 = qo[3 * vol + o], q4 = qo[4 * vol + o];
-#ifdef CHAN_FAST_DIV
+#ifndef CHAN_TRUE_DIV
             const double r = rcp_fast(q0);
             const double u = q1 * r, v = q2 * r, w = q3 * r;
             const double E = q4 * r;
@@ -1425,7 +1427,7 @@ __device__ __forceinline__ void wall_body(const KParams &P, int bx_, int by_, in
             sp[pl][1][by][bx] = u;
             sp[pl][2][by][bx] = v;
             sp[pl][3][by][bx] = w;
-#ifdef CHAN_FAST_DIV
+#ifndef CHAN_TRUE_DIV
             sp[pl][4][by][bx] = (q0 * T) * P.inv_gM2;
 #else
             sp[pl][4][by][bx] = (q0 * T) / P.gM2;
@@ -1548,8 +1550,10 @@ __device__ __forceinline__ void ref_var(const KParams &P, const double *q, int i
     const long long o = (long long)k * P.plane + (long long)j * P.px + i;
     const double q0 = q[o];
     x[0] = q0;
-#ifdef CHAN_FAST_DIV
-    // one reciprocal for the four quotients (within an ulp or two of them)
+#ifndef CHAN_TRUE_DIV
+    // one reciprocal for the four quotients (within an ulp or two of them; the
+    // four true divisions, CHAN_TRUE_DIV, cost 0.65% of the step in this and the
+    // wall kernel)
     const double r = rcp_fast(q0);
     x[1] = q[P.vol + o] * r;
     x[2] = q[2 * P.vol + o] * r;
