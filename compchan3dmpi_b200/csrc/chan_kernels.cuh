@@ -413,7 +413,13 @@ __device__ __forceinline__ float seed_exp2(float x)
 
 __device__ __forceinline__ double rcp_fast(double x)
 {
+#ifdef CHAN_RCP64_SEED
+    // the double-precision hardware approximation as the seed (no conversions)
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+#else
     double r = (double)seed_rcp((float)x);
+#endif
     double e = fma(-x, r, 1.0);
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
@@ -1164,10 +1170,16 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 // kernels, 1% slower in the FP64 one (register allocation), which keeps
                 // the select inside the flux loop.
 #ifdef CHAN_TOP_HOIST_D
-                constexpr bool hoist = true;
+                constexpr bool hoist_d = true;
 #else
-                constexpr bool hoist = sizeof(R) == 4;
+                constexpr bool hoist_d = false;
 #endif
+#ifdef CHAN_NO_TOP_HOIST_F
+                constexpr bool hoist_f = false;
+#else
+                constexpr bool hoist_f = true;
+#endif
+                constexpr bool hoist = sizeof(R) == 8 ? hoist_d : hoist_f;
                 if (hoist && top) {
 #pragma unroll
                     for (int c = 0; c < 4; c++) hp1[c] = (R)P.hwt[c * plane + colo];
