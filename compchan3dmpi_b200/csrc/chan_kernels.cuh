@@ -379,17 +379,16 @@ __device__ __forceinline__ int wrap_idx(int i, int n)
 
 // ---------------------------------------------------------------------------
 // Short math for the transport law mu = k = T^0.7 (main_v1.9.f90:643, 720) and
-// for 1/rho.  Both start from the single-precision hardware approximations
-// and refine in FP64.
+// for 1/rho.  Both start from hardware approximations and refine in FP64.
 //
-// rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from a
-// float seed (relative error 2^-23 -> ~1e-14 -> ~1 ulp).  Valid for |x| in
-// the float normal range, which covers rho and mu of any physical state.
-// The float seeds are the hardware approximations themselves (rcp.approx,
-// ex2.approx; relative errors about 2^-23 and 2^-22), which the FP64
-// refinement takes to the same accuracy.  Seeding from the correctly rounded
-// float reciprocal and the float library exp2 instead (CHAN_EXACT_SEEDS) made
-// the FP64 stage kernel 7.5% slower and the float one 2.7%.
+// The seeds are the approximations themselves: rcp.approx.ftz.f64 for the
+// reciprocal, ex2.approx.ftz.f32 (after lg2.approx) for the power.  The FP64
+// refinement squares (Newton) or cubes (Halley) the seed's relative error at
+// each step, so it reaches the same accuracy from them as from exact float
+// values.  Measured against the alternatives on the FP64 stage kernel: the
+// correctly rounded float reciprocal __frcp_rn and the library exp2f
+// (CHAN_EXACT_SEEDS) 7.5% slower; the float reciprocal approximation with its
+// two conversions (CHAN_F32_RCP_SEED) 1.2% slower.
 __device__ __forceinline__ float seed_rcp(float x)
 {
 #ifndef CHAN_EXACT_SEEDS
@@ -411,10 +410,12 @@ __device__ __forceinline__ float seed_exp2(float x)
 #endif
 }
 
+// rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from the seed
+// (to about 1 ulp).  Valid for |x| in the normal range, which covers rho and mu
+// of any physical state.
 __device__ __forceinline__ double rcp_fast(double x)
 {
-#ifdef CHAN_RCP64_SEED
-    // the double-precision hardware approximation as the seed (no conversions)
+#if !defined(CHAN_F32_RCP_SEED) && !defined(CHAN_EXACT_SEEDS)
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
 #else
