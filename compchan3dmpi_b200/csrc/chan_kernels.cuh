@@ -399,6 +399,16 @@ __device__ __forceinline__ float seed_rcp(float x)
     return __frcp_rn(x);
 #endif
 }
+__device__ __forceinline__ float seed_log2(float x)
+{
+#ifdef CHAN_LG2_FTZ
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return __log2f(x);
+#endif
+}
 __device__ __forceinline__ float seed_exp2(float x)
 {
 #ifndef CHAN_EXACT_SEEDS
@@ -435,7 +445,7 @@ __device__ __forceinline__ double rcp_fast(double x)
 __device__ __forceinline__ double pow07(double T)
 {
     const float tf = (float)T;
-    double y = (double)seed_exp2(0.7f * __log2f(tf));
+    double y = (double)seed_exp2(0.7f * seed_log2(tf));
     const double T2 = T * T, T4 = T2 * T2, a = (T4 * T2) * T;
     const double y2 = y * y, y4 = y2 * y2, y8 = y4 * y4, u = y8 * y2;
     const double num = fma(9.0, u, 11.0 * a);
@@ -970,6 +980,19 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // plane); own column of t+2; (float rings: the own point's RK base
         // starts its way into shared memory); plane t+1's box is converted
         if (t < ke) issue(t + 2, iN);
+#ifdef CHAN_PREFETCH_BOX_L1
+        // per-thread box loads (the stage whose input is wider than its rings):
+        // plane t+2's box into L1 now, converted at the next plane
+        if (!TMA && t + 2 <= n3) {
+#pragma unroll
+            for (int l = 0; l < NL; l++) {
+                if (lp[l] < 0) continue;
+                const QI *src = qin() + (long long)(t + 2) * plane + lo[l];
+#pragma unroll
+                for (int v = 0; v < 5; v++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + v * vol));
+            }
+        }
+#endif
         const bool need_base = P.rk_mode != 0;
         if (S::tma_base && need_base) issue_base(t);
         if (S::prefetch_base) {
