@@ -382,7 +382,7 @@ __device__ __forceinline__ int wrap_idx(int i, int n)
 // for 1/rho.  Both start from hardware approximations and refine in FP64.
 //
 // The seeds are the approximations themselves: rcp.approx.ftz.f64 for the
-// reciprocal, ex2.approx.ftz.f32 (after lg2.approx) for the power.  The FP64
+// reciprocal, ex2.approx.ftz.f32 after lg2.approx.ftz.f32 for the power.  The FP64
 // refinement squares (Newton) or cubes (Halley) the seed's relative error at
 // each step, so it reaches the same accuracy from them as from exact float
 // values.  Measured against the alternatives on the FP64 stage kernel: the
@@ -401,13 +401,9 @@ __device__ __forceinline__ float seed_rcp(float x)
 }
 __device__ __forceinline__ float seed_log2(float x)
 {
-#ifdef CHAN_LG2_FTZ
     float r;
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
-#else
-    return __log2f(x);
-#endif
 }
 __device__ __forceinline__ float seed_exp2(float x)
 {
@@ -581,9 +577,7 @@ __device__ __forceinline__ float mu_of<float>(double T)
     // inside the float path's own rounding); the library log2f/exp2f cost 2.5% of
     // the float stage kernel (CHAN_LIBM_MU_F)
 #ifndef CHAN_LIBM_MU_F
-    float l;
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"((float)T));
-    return seed_exp2(0.7f * l);
+    return seed_exp2(0.7f * seed_log2((float)T));
 #else
     return exp2f(0.7f * log2f((float)T));
 #endif
@@ -980,19 +974,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // plane); own column of t+2; (float rings: the own point's RK base
         // starts its way into shared memory); plane t+1's box is converted
         if (t < ke) issue(t + 2, iN);
-#ifdef CHAN_PREFETCH_BOX_L1
-        // per-thread box loads (the stage whose input is wider than its rings):
-        // plane t+2's box into L1 now, converted at the next plane
-        if (!TMA && t + 2 <= n3) {
-#pragma unroll
-            for (int l = 0; l < NL; l++) {
-                if (lp[l] < 0) continue;
-                const QI *src = qin() + (long long)(t + 2) * plane + lo[l];
-#pragma unroll
-                for (int v = 0; v < 5; v++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + v * vol));
-            }
-        }
-#endif
         const bool need_base = P.rk_mode != 0;
         if (S::tma_base && need_base) issue_base(t);
         if (S::prefetch_base) {
