@@ -1018,12 +1018,24 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             for (int c = 0; c < 5; c++) qp2[c] = (R)qc[c];
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
+#elif defined(CHAN_LATE_T2)
+        // own column of plane t+2 into L1 now; loaded and converted in phase C,
+        // where its values start to be used
+        if (col_ok && t + 2 <= n3) {
+            const QI *src = qin() + (long long)(t + 2) * plane + colo;
+#pragma unroll
+            for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+        }
+        bad = !wait_slot(iP);
+        convert(t + 1, iP, pP, mP);
 #else
         if (col_ok && t + 2 <= n3) {
             double q[5], u, v, w, T;
             center(t + 2, q, u, v, w, T);
+#ifndef CHAN_LATE_QP2
 #pragma unroll
             for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
+#endif
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
         bad = !wait_slot(iP);
@@ -1039,6 +1051,15 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             const R czt = ktab<R>(P, 0, t);
             const R *MU = smu(mZ), *PR = spr(mZ, iZ);
             if (col_ok) {
+#ifdef CHAN_LATE_T2
+                if (t + 2 <= n3) {
+                    double q[5], u, v, w, T;
+                    center(t + 2, q, u, v, w, T);
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
+                    up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
+                }
+#endif
                 if (t + 1 != n3)
                     hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 R g[4];
@@ -1167,6 +1188,14 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                     inv_weights(wm2, wm1, w0, wp1, wp2, qk, ktab<R>(P, 1, t), ktab<R>(P, 2, t), w);
                 }
                 const R czt = ktab<R>(P, 0, t);
+#ifdef CHAN_LATE_QP2
+                // plane t+2's own-column Q again (in L1 since phase A)
+                if (t + 2 <= n3) {
+                    const long long off = (long long)(t + 2) * plane + colo;
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qp2[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
+                }
+#endif
                 Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
                 // float rings: the top plane's hD from the prologue's staging, under one
