@@ -511,6 +511,14 @@ struct StageShape {
     static constexpr bool tma_base = false;
 #endif
     static constexpr bool fx_shfl = tma_base;
+    // where the own column of plane t+2 is read (measured per ring type: the FP64
+    // kernel 7% faster reading its Q twice than holding it in registers, whose
+    // spills it removes; the float kernels 2-3% faster loading it in phase C)
+#ifdef CHAN_EARLY_T2
+    static constexpr bool late_t2 = false, late_qp2 = false;
+#else
+    static constexpr bool late_t2 = sizeof(R) == 4, late_qp2 = sizeof(R) == 8;
+#endif
     static constexpr int NFX = fx_shfl ? 2 * TJ : TJ * (TI + 2), NGY = (TJ + 2) * TI;
     // float rings keep mu only and form p from rho and T where it is used;
     // FP64 rings keep (mu, p) unless the RK base takes the room
@@ -668,6 +676,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 {
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
+    // the mixed path's first stage (double in, float rings; per-thread box loads)
+#ifdef CHAN_S1_LATE_QP2
+    constexpr bool s1 = std::is_same<QI, double>::value && sizeof(R) == 4;
+    constexpr bool late_t2 = S::late_t2 && !s1, late_qp2 = S::late_qp2 || s1;
+#else
+    constexpr bool late_t2 = S::late_t2, late_qp2 = S::late_qp2;
+#endif
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT, MPW = S::MPW, QSLOT = S::QSLOT;
     // boxes by bulk tensor copy when the input is stored in the ring type
 #ifdef CHAN_NO_TMA
@@ -1018,24 +1033,24 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             for (int c = 0; c < 5; c++) qp2[c] = (R)qc[c];
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
-#elif defined(CHAN_LATE_T2)
-        // own column of plane t+2 into L1 now; loaded and converted in phase C,
-        // where its values start to be used
-        if (col_ok && t + 2 <= n3) {
-            const QI *src = qin() + (long long)(t + 2) * plane + colo;
-#pragma unroll
-            for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
-        }
-        bad = !wait_slot(iP);
-        convert(t + 1, iP, pP, mP);
 #else
-        if (col_ok && t + 2 <= n3) {
+        // plane t+2's own column: the float kernels prefetch it into L1 here and
+        // load and convert it in phase C, where its values start to be used; the
+        // FP64 kernel loads and converts it here but reads its Q again in phase E
+        // (an L1 hit) instead of keeping it in registers across the plane
+        if (late_t2) {
+            if (col_ok && t + 2 <= n3) {
+                const QI *src = qin() + (long long)(t + 2) * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+            }
+        } else if (col_ok && t + 2 <= n3) {
             double q[5], u, v, w, T;
             center(t + 2, q, u, v, w, T);
-#ifndef CHAN_LATE_QP2
+            if (!late_qp2) {
 #pragma unroll
-            for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
-#endif
+                for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
+            }
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
         bad = !wait_slot(iP);
@@ -1051,15 +1066,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             const R czt = ktab<R>(P, 0, t);
             const R *MU = smu(mZ), *PR = spr(mZ, iZ);
             if (col_ok) {
-#ifdef CHAN_LATE_T2
-                if (t + 2 <= n3) {
+                if (late_t2 && t + 2 <= n3) {
                     double q[5], u, v, w, T;
                     center(t + 2, q, u, v, w, T);
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
                     up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
                 }
-#endif
                 if (t + 1 != n3)
                     hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
                 R g[4];
@@ -1188,14 +1201,12 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                     inv_weights(wm2, wm1, w0, wp1, wp2, qk, ktab<R>(P, 1, t), ktab<R>(P, 2, t), w);
                 }
                 const R czt = ktab<R>(P, 0, t);
-#ifdef CHAN_LATE_QP2
                 // plane t+2's own-column Q again (in L1 since phase A)
-                if (t + 2 <= n3) {
+                if (late_qp2 && t + 2 <= n3) {
                     const long long off = (long long)(t + 2) * plane + colo;
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
                 }
-#endif
                 Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
                 // float rings: the top plane's hD from the prologue's staging, under one
