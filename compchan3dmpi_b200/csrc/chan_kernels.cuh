@@ -676,13 +676,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 {
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
-    // the mixed path's first stage (double in, float rings; per-thread box loads)
-#ifdef CHAN_S1_LATE_QP2
-    constexpr bool s1 = std::is_same<QI, double>::value && sizeof(R) == 4;
-    constexpr bool late_t2 = S::late_t2 && !s1, late_qp2 = S::late_qp2 || s1;
-#else
     constexpr bool late_t2 = S::late_t2, late_qp2 = S::late_qp2;
-#endif
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT, MPW = S::MPW, QSLOT = S::QSLOT;
     // boxes by bulk tensor copy when the input is stored in the ring type
 #ifdef CHAN_NO_TMA
