@@ -677,15 +677,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     using S = StageShape<TI, TJ, R>;
     using Slot = SlotT<R>;
     constexpr bool late_t2 = S::late_t2, late_qp2 = S::late_qp2;
-#if defined(CHAN_LATE_QM_F)
-    constexpr bool late_qm = true;
-#elif defined(CHAN_LATE_QM)
-    // FP64: Q of planes t-1 and t-2 at the own column read in the update (from L1,
-    // prefetched in phase A) instead of carried in registers from plane to plane
-    constexpr bool late_qm = sizeof(R) == 8;
-#else
-    constexpr bool late_qm = false;
-#endif
     constexpr int BX = S::BX, BY = S::BY, NB = S::NB, NT = S::NT, MPW = S::MPW, QSLOT = S::QSLOT;
     // boxes by bulk tensor copy when the input is stored in the ring type
 #ifdef CHAN_NO_TMA
@@ -992,14 +983,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // plane); own column of t+2; (float rings: the own point's RK base
         // starts its way into shared memory); plane t+1's box is converted
         if (t < ke) issue(t + 2, iN);
-        if (late_qm && out_ok) {
-            const QI *src = qin() + (long long)(t - 1) * plane + colo;
-#pragma unroll
-            for (int c = 0; c < 5; c++) {
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
-                if (t - 2 >= 1) asm volatile("prefetch.global.L1 [%0];" ::"l"(src - plane + c * vol));
-            }
-        }
         const bool need_base = P.rk_mode != 0;
         if (S::tma_base && need_base) issue_base(t);
         if (S::prefetch_base) {
@@ -1218,21 +1201,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
                 }
-                R qa[5], qb[5];   // Q at t-2 and t-1
-#pragma unroll
-                for (int c = 0; c < 5; c++) {
-                    qa[c] = qm2[c];
-                    qb[c] = qm1[c];
-                }
-                if (late_qm) {
-                    const long long off = (long long)(t - 1) * plane + colo;
-#pragma unroll
-                    for (int c = 0; c < 5; c++) {
-                        qb[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
-                        qa[c] = t - 2 >= 1 ? (R)ldq_c<PERSIST>(qin() + c * vol + off - plane) : R(0);
-                    }
-                }
-                Fs[0] = Fs[0] + wsum(w, qa[0], qb[0], q0[0], sq(iP, 0)[bc], qp2[0]);
+                Fs[0] = Fs[0] + wsum(w, qm2[0], qm1[0], q0[0], sq(iP, 0)[bc], qp2[0]);
                 const bool top = t + 1 == n3;   // hD of the top wall plane was staged in the prologue
                 // float rings: the top plane's hD from the prologue's staging, under one
                 // uniform branch (hp1 is not formed on the top plane, and the march ends
@@ -1256,7 +1225,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
 #pragma unroll
                 for (int c = 1; c < 5; c++) {
-                    const R H1 = wsum(w, qa[c], qb[c], q0[c], sq(iP, c)[bc], qp2[c]);
+                    const R H1 = wsum(w, qm2[c], qm1[c], q0[c], sq(iP, c)[bc], qp2[c]);
                     const R hp = hoist ? hp1[c - 1] : (top ? (R)P.hwt[(c - 1) * plane + colo] : hp1[c - 1]);
                     const R H2 = (hp - hm1[c - 1]) * czt;
                     Fs[c] = (Fs[c] + H1) + H2;
