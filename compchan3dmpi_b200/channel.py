@@ -239,7 +239,7 @@ class Channel:
         self._check(self.L.chan_set_buoyancy(self._h, float(Ri), float(Tref)))
 
     def set_launch(self, tile: int = 0, nchunks: int = 0):
-        """Stage-kernel launch shape: tile 0 (32x8), 1 (32x4) or 2 (16x16), k-chunks (0: automatic)."""
+        """Stage-kernel launch shape: tile 0 (32x8), 1 (32x4), 2 (16x16) or 3 (32x16), k-chunks (0: automatic)."""
         self._check(self.L.chan_set_launch(self._h, int(tile), int(nchunks)))
 
     def launch(self):
