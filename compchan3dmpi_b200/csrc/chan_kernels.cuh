@@ -812,9 +812,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         R *MU = smu(mo), *PR = sMP + mo + NB;
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
-#pragma unroll
-        for (int l = 0; l < NL; l++) {
-            if (lp[l] < 0) continue;
+        auto one = [&](int l, bool wall_plane) {
+            if (lp[l] < 0) return;
             const int p = lp[l] & 0xffff;
             const bool r1 = (lp[l] & 0x10000) != 0;
             double q[5];
@@ -828,7 +827,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
             double u, vv, w, T, pr;
             R mu;
-            if (wall) {
+            if (wall_plane) {
                 const int bj = p / BX, bi = p - bj * BX;
                 const long long wo = (long long)wrap_idx(j0 - 2 + bj, n2) * P.px + wrap_idx(i0 - 2 + bi, n1);
                 u = W[1 * plane + wo];
@@ -854,7 +853,22 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 MU[p] = mu;
                 if (S::p_ring) PR[p] = (R)pr;
             }
-        }
+        };
+        // the wall test taken once per plane, so that each loop's body is
+        // straight-line code (2.6% of the FP64 stage time against one loop with the
+        // test inside); the per-thread box loads one box point at a time, with fewer
+        // loads in flight (0.4% of the mean float stage time)
+        auto loop = [&](bool wall_plane) {
+            if (!TMA) {
+#pragma unroll 1
+                for (int l = 0; l < NL; l++) one(l, wall_plane);
+            } else {
+#pragma unroll
+                for (int l = 0; l < NL; l++) one(l, wall_plane);
+            }
+        };
+        if (wall) loop(true);
+        else loop(false);
     };
 
     // own-column Q and u,v,w,T of plane m read straight from memory
