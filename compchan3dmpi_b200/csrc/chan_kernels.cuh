@@ -1078,7 +1078,9 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                     double q[5], u, v, w, T;
                     center(t + 2, q, u, v, w, T);
 #pragma unroll
+#ifndef CHAN_RELOAD_QP2_F
                     for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
+#endif
                     up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
                 }
                 if (t + 1 != n3)
@@ -1210,7 +1212,11 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
                 const R czt = ktab<R>(P, 0, t);
                 // plane t+2's own-column Q again (in L1 since phase A)
+#ifdef CHAN_RELOAD_QP2_F
+                if ((late_qp2 || late_t2) && t + 2 <= n3) {
+#else
                 if (late_qp2 && t + 2 <= n3) {
+#endif
                     const long long off = (long long)(t + 2) * plane + colo;
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
