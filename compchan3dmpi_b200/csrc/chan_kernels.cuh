@@ -1077,8 +1077,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 if (late_t2 && t + 2 <= n3) {
                     double q[5], u, v, w, T;
                     center(t + 2, q, u, v, w, T);
-#pragma unroll
 #ifndef CHAN_RELOAD_QP2_F
+#pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
 #endif
                     up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
