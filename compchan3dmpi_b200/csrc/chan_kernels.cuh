@@ -516,6 +516,8 @@ struct StageShape {
     // spills it removes; the float kernels 2-3% faster loading it in phase C)
 #ifdef CHAN_EARLY_T2
     static constexpr bool late_t2 = false, late_qp2 = false;
+#elif defined(CHAN_D_T2)
+    static constexpr bool late_t2 = true, late_qp2 = sizeof(R) == 8;
 #else
     static constexpr bool late_t2 = sizeof(R) == 4, late_qp2 = sizeof(R) == 8;
 #endif
