@@ -516,8 +516,6 @@ struct StageShape {
     // spills it removes; the float kernels 2-3% faster loading it in phase C)
 #ifdef CHAN_EARLY_T2
     static constexpr bool late_t2 = false, late_qp2 = false;
-#elif defined(CHAN_D_T2)
-    static constexpr bool late_t2 = true, late_qp2 = sizeof(R) == 8;
 #else
     static constexpr bool late_t2 = sizeof(R) == 4, late_qp2 = sizeof(R) == 8;
 #endif
@@ -1079,10 +1077,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 if (late_t2 && t + 2 <= n3) {
                     double q[5], u, v, w, T;
                     center(t + 2, q, u, v, w, T);
-#ifndef CHAN_RELOAD_QP2_F
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
-#endif
                     up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
                 }
                 if (t + 1 != n3)
@@ -1214,11 +1210,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
                 const R czt = ktab<R>(P, 0, t);
                 // plane t+2's own-column Q again (in L1 since phase A)
-#ifdef CHAN_RELOAD_QP2_F
-                if ((late_qp2 || late_t2) && t + 2 <= n3) {
-#else
                 if (late_qp2 && t + 2 <= n3) {
-#endif
                     const long long off = (long long)(t + 2) * plane + colo;
 #pragma unroll
                     for (int c = 0; c < 5; c++) qp2[c] = (R)ldq_c<PERSIST>(qin() + c * vol + off);
