@@ -1016,6 +1016,14 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
 #endif
+#ifdef CHAN_PREFETCH_T3
+        // plane t+3's own column into L1 a plane before it is loaded
+        if (col_ok && t + 3 <= n3) {
+            const QI *src = qin() + (long long)(t + 3) * plane + colo;
+#pragma unroll
+            for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+        }
+#endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
 #ifdef CHAN_LATE_CENTER
         // own column of plane t+2: loads issued now, primitives formed after the
