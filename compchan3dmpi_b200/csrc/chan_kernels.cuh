@@ -1016,40 +1016,15 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
 #endif
-#ifdef CHAN_PREFETCH_T3
-        // plane t+3's own column into L1 a plane before it is loaded
-        if (col_ok && t + 3 <= n3) {
+        // FP64: plane t+3's own column into L1 a plane before it is loaded (1.8% of the
+        // FP64 stage time; the float kernels, which load plane t+2 in phase C, are
+        // slower with it)
+        if (sizeof(R) == 8 && col_ok && t + 3 <= n3) {
             const QI *src = qin() + (long long)(t + 3) * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
-#endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
-#ifdef CHAN_LATE_CENTER
-        // own column of plane t+2: loads issued now, primitives formed after the
-        // box conversion, so that the loads' latency overlaps it
-        double qc[5] = {0, 0, 0, 0, 0};
-        const bool c2 = col_ok && t + 2 <= n3;
-        if (c2) {
-            const long long off = (long long)(t + 2) * plane + colo;
-#pragma unroll
-            for (int c = 0; c < 5; c++) qc[c] = ldq_c<PERSIST>(qin() + c * vol + off);
-        }
-        bad = !wait_slot(iP);
-        convert(t + 1, iP, pP, mP);
-        if (c2) {
-            double u, v, w, T;
-            if (t + 2 == n3) {
-                const double *W = P.wp + (size_t)8 * plane + colo;
-                u = W[1 * plane]; v = W[2 * plane]; w = W[3 * plane]; T = W[5 * plane];
-            } else {
-                prims_from_q(P, qc, u, v, w, T);
-            }
-#pragma unroll
-            for (int c = 0; c < 5; c++) qp2[c] = (R)qc[c];
-            up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
-        }
-#else
         // plane t+2's own column: the float kernels prefetch it into L1 here and
         // load and convert it in phase C, where its values start to be used; the
         // FP64 kernel loads and converts it here but reads its Q again in phase E
@@ -1071,7 +1046,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         }
         bad = !wait_slot(iP);
         convert(t + 1, iP, pP, mP);
-#endif
         if (__syncthreads_or(bad)) { give_up(); return; }
 
         // ---------- C: viscous flux vectors
