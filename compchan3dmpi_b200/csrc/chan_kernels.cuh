@@ -1024,6 +1024,26 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
+#ifdef CHAN_PREFETCH_TABLES
+        // next plane's per-plane coefficients and forcing density into L1 (one lane each)
+        if (t < ke && tid < 6) {
+            const double *a = tid == 0 ? P.czh : (tid == 1 ? P.cz8 : (tid == 2 ? P.cz12 : (tid == 3 ? P.pez : P.stat)));
+            const int k = tid == 4 ? t : (tid == 5 ? t + 2 : t + 1);
+            if (tid != 5 || t + 2 <= n3) asm volatile("prefetch.global.L1 [%0];" ::"l"(tid == 5 ? P.czh + k : a + k));
+        }
+#endif
+#ifdef CHAN_PREFETCH_BOX_L1
+        // per-thread box loads: plane t+2's box into L1 now, converted at the next plane
+        if (!TMA && t + 2 <= n3) {
+#pragma unroll
+            for (int l = 0; l < NL; l++) {
+                if (lp[l] < 0) continue;
+                const QI *src = qin() + (long long)(t + 2) * plane + lo[l];
+#pragma unroll
+                for (int v = 0; v < 5; v++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + v * vol));
+            }
+        }
+#endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
         // plane t+2's own column: the float kernels prefetch it into L1 here and
         // load and convert it in phase C, where its values start to be used; the
