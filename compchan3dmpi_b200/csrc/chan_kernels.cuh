@@ -1011,9 +1011,23 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // the own point's RK base into L1 now; the update reads it at the end of
         // the plane (2.7% of the FP64 stage time against loading it there cold)
         if (!S::prefetch_base && !S::tma_base && P.rk_mode != 0 && out_ok) {
+#ifdef CHAN_PREFETCH_BASE_AHEAD
+            // a plane ahead: plane t+1's base now (plane kb's at the chunk's first plane)
+            if (t == kb) {
+                const double *src0 = P.qbase + (long long)t * plane + colo;
+#pragma unroll
+                for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src0 + c * vol));
+            }
+            const double *src = P.qbase + (long long)(t + 1) * plane + colo;
+            if (t < ke) {
+#pragma unroll
+                for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+            }
+#else
             const double *src = P.qbase + (long long)t * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
+#endif
         }
 #endif
         // FP64: plane t+3's own column into L1 a plane before it is loaded (1.8% of the
