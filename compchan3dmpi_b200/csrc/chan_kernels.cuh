@@ -416,9 +416,10 @@ __device__ __forceinline__ float seed_exp2(float x)
 #endif
 }
 
-// rcp_fast: Newton-Raphson for 1/x, r <- r + r*(1 - x*r), twice from the seed
-// (to about 1 ulp).  Valid for |x| in the normal range, which covers rho and mu
-// of any physical state.
+// rcp_fast: 1/x from the seed r by one third-order step, r (1 + e + e^2) with
+// e = 1 - x r (the seed's error cubed: to about 1 ulp), one dependent FMA fewer
+// than two Newton steps (CHAN_RCP_NEWTON2; 0.5% of the FP64 stage time).  Valid
+// for |x| in the normal range, which covers rho and mu of any physical state.
 __device__ __forceinline__ double rcp_fast(double x)
 {
 #if !defined(CHAN_F32_RCP_SEED) && !defined(CHAN_EXACT_SEEDS)
@@ -427,19 +428,40 @@ __device__ __forceinline__ double rcp_fast(double x)
 #else
     double r = (double)seed_rcp((float)x);
 #endif
+#ifndef CHAN_RCP_NEWTON2
+    // one step of third order: 1/x = r / (1 - e) = r (1 + e + e^2 + ...), e = 1 - x r
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+#else
     double e = fma(-x, r, 1.0);
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
+#endif
 }
 
-// pow07: y = T^0.7 is the positive root of y^10 = T^7.  One Halley step for
-// f(y) = y^10 - a, a = T^7:  y <- y * (9 y^10 + 11 a) / (11 y^10 + 9 a),
-// cubic convergence from a float seed exp2(0.7*log2 T) (relative error
-// ~3e-7 -> ~1e-19), so the result is limited by FP64 rounding (~2 ulp).
-// T <= 0 gives NaN, as the reference's T**0.7 would.
+// pow07: y = T^0.7 = T x with x = T^-0.3, the positive root of x^10 T^3 = 1.
+// From the float seed x0 = exp2(-0.3 log2 T) (relative error ~3e-7),
+// e = 1 - x0^10 T^3 (~3e-6) and x = x0 (1 - e)^(-1/10), whose binomial series
+// 1 + e/10 + 0.055 e^2 + ... is cut after e^2 (the rest ~1e-18): twelve FP64
+// operations and no division, so the result is limited by FP64 rounding
+// (~2 ulp).  The earlier form, one Halley step on y^10 = T^7 with a reciprocal
+// (CHAN_POW_HALLEY), takes 0.4% more of the FP64 stage time.  T <= 0 gives NaN
+// (the reference's T**0.7 does for T < 0; T = 0 does not arise).
 __device__ __forceinline__ double pow07(double T)
 {
+#ifndef CHAN_POW_HALLEY
+    // y = T * x with x = T^-0.3, the root of x^10 T^3 = 1.  From the float seed
+    // x0 (relative error ~3e-7), e = 1 - x0^10 T^3 and
+    // x = x0 (1 - e)^(-1/10) = x0 (1 + e/10 + 0.055 e^2 + 0.0385 e^3 + ...):
+    // the series to e^2 leaves ~1e-18; no division.
+    const double x0 = (double)seed_exp2(-0.3f * seed_log2((float)T));
+    const double t2 = T * T, t3 = t2 * T;
+    const double x2 = x0 * x0, x4 = x2 * x2, x8 = x4 * x4, x10 = x8 * x2;
+    const double e = fma(-x10, t3, 1.0);
+    const double pe = fma(fma(0.0385, e, 0.055), e, 0.1);
+    return T * fma(x0 * e, pe, x0);
+#else
     const float tf = (float)T;
     double y = (double)seed_exp2(0.7f * seed_log2(tf));
     const double T2 = T * T, T4 = T2 * T2, a = (T4 * T2) * T;
@@ -447,6 +469,7 @@ __device__ __forceinline__ double pow07(double T)
     const double num = fma(9.0, u, 11.0 * a);
     const double den = fma(11.0, u, 9.0 * a);
     return (y * num) * rcp_fast(den);
+#endif
 }
 
 // primitives of one point from the conservative state (calcPrim, main_v1.9.f90:600-609)
@@ -799,6 +822,35 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         lo[l] = gj * P.px + gi;
     }
 
+    // The inviscid x and y flux derivatives of plane t (F1 + G1) need only plane
+    // t's Q box and u, v, which the previous plane converted: they are formed in
+    // phase A, in the same straight-line block as the conversion of plane t+1's
+    // box, whose dependency chains (reciprocal, power) they fill (1.7% of the
+    // FP64 stage time, 2.4% of the float one, against forming them in phase E;
+    // in phase C, beside the viscous fluxes, they were 2.8% slower than in E).
+    // CHAN_XY_IN_E keeps them in phase E, for measurement.
+#ifdef CHAN_XY_IN_E
+    constexpr bool xy_a = false;
+#else
+    constexpr bool xy_a = true;
+#endif
+    R Fxy[5] = {0, 0, 0, 0, 0};
+    auto inv_xy = [&]() {
+        const R mu0 = smu(mZ)[bc];
+        const R *U = sPr + pZ, *V = sPr + pZ + NB;
+        const bool qx = (C.pex * fabs(sq(iZ, 1)[bc])) > C.PexVal * mu0;
+        const bool qy = (C.pey * fabs(sq(iZ, 2)[bc])) > C.PeyVal * mu0;
+        R wx[5], wy[5];
+        inv_weights(U[bc - 2], U[bc - 1], U[bc], U[bc + 1], U[bc + 2], qx, C.sx8, C.sx12, wx);
+        inv_weights(V[bc - 2 * BX], V[bc - BX], V[bc], V[bc + BX], V[bc + 2 * BX], qy, C.sy8, C.sy12, wy);
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+            const R *Q = sq(iZ, c);
+            Fxy[c] = wsum(wx, Q[bc - 2], Q[bc - 1], Q[bc], Q[bc + 1], Q[bc + 2]) +
+                     wsum(wy, Q[bc - 2 * BX], Q[bc - BX], Q[bc], Q[bc + BX], Q[bc + 2 * BX]);
+        }
+    };
+
     // primitives (and mu, p on R1) of plane m over the box, from its Q box in
     // slot s (with per-thread loads, Q is first loaded into the slot).  A wall
     // plane's box holds, at periodic duplicates and ghosts, the values of their
@@ -807,7 +859,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     // flux of its image (whose wall values may differ from the duplicate's own
     // under a non-periodic wall BC).  hD on a wall plane reads the wall's own
     // values from memory instead (hflux_wall).
-    auto convert = [&](int m, int s, int po, int mo) {
+    auto no_extra = []() {};
+    auto convert = [&](int m, int s, int po, int mo, bool with_xy, auto &&extra) {
         const Slot sl = slot(po);
         R *MU = smu(mo), *PR = sMP + mo + NB;
         const bool wall = (m == 1 || m == n3);
@@ -866,6 +919,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
                 for (int l = 0; l < NL; l++) one(l, wall_plane);
             }
+            if (xy_a && with_xy) inv_xy();
+            extra();
         };
         if (wall) loop(true);
         else loop(false);
@@ -939,9 +994,9 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     issue(kb, 1);
     issue(kb + 1, 2);   // kb+1 <= ke+1 <= nP3
     bool bad = !wait_slot(0);
-    convert(kb - 1, 0, pP, mP);
+    convert(kb - 1, 0, pP, mP, false, no_extra);
     bad = !wait_slot(1) || bad;
-    convert(kb, 1, pZ, mZ);
+    convert(kb, 1, pZ, mZ, false, no_extra);
     if (__syncthreads_or(bad)) { give_up(); return; }
 
     R qm2[5] = {0, 0, 0, 0, 0}, qm1[5], hm1[4] = {0, 0, 0, 0}, h0[4] = {0, 0, 0, 0};
@@ -1059,6 +1114,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         }
 #endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
+#ifdef CHAN_T2_SPLIT
+        constexpr bool t2_split = !late_t2;
+#else
+        constexpr bool t2_split = false;
+#endif
+        const bool c2 = col_ok && t + 2 < n3;
+        double cq[5] = {0, 0, 0, 0, 0};
         // plane t+2's own column: the float kernels prefetch it into L1 here and
         // load and convert it in phase C, where its values start to be used; the
         // FP64 kernel loads and converts it here but reads its Q again in phase E
@@ -1069,6 +1131,11 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
                 for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
             }
+        } else if (t2_split && c2) {
+            // interior plane t+2: its own column's Q now, its primitives after the box wait
+            const long long off = (long long)(t + 2) * plane + colo;
+#pragma unroll
+            for (int c = 0; c < 5; c++) cq[c] = ldq_c<PERSIST>(qin() + c * vol + off);
         } else if (col_ok && t + 2 <= n3) {
             double q[5], u, v, w, T;
             center(t + 2, q, u, v, w, T);
@@ -1078,8 +1145,24 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
             up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
         }
+        // the primitives of plane t+2's own column formed in the same straight-line
+        // block as the box conversion (selects keep the other cases' values)
+        auto t2_prims = [&]() {
+            if (t2_split) {
+                double u, v, w, T;
+                prims_from_q(P, cq, u, v, w, T);
+                up2 = c2 ? (R)u : up2;
+                vp2 = c2 ? (R)v : vp2;
+                wp2 = c2 ? (R)w : wp2;
+                Tp2 = c2 ? (R)T : Tp2;
+                if (!late_qp2) {
+#pragma unroll
+                    for (int c = 0; c < 5; c++) qp2[c] = c2 ? (R)cq[c] : qp2[c];
+                }
+            }
+        };
         bad = !wait_slot(iP);
-        convert(t + 1, iP, pP, mP);
+        convert(t + 1, iP, pP, mP, true, t2_prims);
         if (__syncthreads_or(bad)) { give_up(); return; }
 
         // ---------- C: viscous flux vectors
@@ -1168,8 +1251,25 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #endif
             R Fs[5];   // sum of the flux derivatives
             const R mu0 = smu(mZ)[bc];
+            if (xy_a) {
+                // (F1 + G1) from phase A, then the viscous x and y terms
+                Fs[0] = Fxy[0];
+#pragma unroll
+                for (int c = 1; c < 5; c++) {
+                    R F2;
+                    if (S::fx_shfl) {
+                        F2 = (fxp[c - 1] - fxm[c - 1]) * C.hdx;
+                    } else {
+                        const int r = (c - 1) * TJ + ty;
+                        F2 = (sF[r * (TI + 2) + tx + 2] - sF[r * (TI + 2) + tx]) * C.hdx;
+                    }
+                    const R G2 = (sG[((c - 1) * (TJ + 2) + ty + 2) * TI + tx] -
+                                  sG[((c - 1) * (TJ + 2) + ty) * TI + tx]) * C.hdy;
+                    Fs[c] = (Fxy[c] + F2) + G2;
+                }
+            }
             // x
-            {
+            if (!xy_a) {
                 const R *U = s0.U;
                 const bool qk = (C.pex * fabs(q0[1])) > C.PexVal * mu0;
                 R w[5];
@@ -1194,7 +1294,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
             }
             // y
-            {
+            if (!xy_a) {
                 const R *V = s0.V;
                 const bool qk = (C.pey * fabs(q0[2])) > C.PeyVal * mu0;
                 R w[5];
