@@ -537,8 +537,10 @@ struct StageShape {
     // where the own column of plane t+2 is read (measured per ring type: the FP64
     // kernel 7% faster reading its Q twice than holding it in registers, whose
     // spills it removes; the float kernels 2-3% faster loading it in phase C)
-#ifdef CHAN_EARLY_T2
+#if defined(CHAN_EARLY_T2)
     static constexpr bool late_t2 = false, late_qp2 = false;
+#elif defined(CHAN_T2_SPLIT_F)
+    static constexpr bool late_t2 = false, late_qp2 = true;
 #else
     static constexpr bool late_t2 = sizeof(R) == 4, late_qp2 = sizeof(R) == 8;
 #endif
@@ -1048,10 +1050,25 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     __syncthreads();
 
     for (int t = kb; t <= ke; t++) {
-        // ---------- A: plane t+2's box starts its way in (converted at the next
-        // plane); own column of t+2; (float rings: the own point's RK base
-        // starts its way into shared memory); plane t+1's box is converted
-        if (t < ke) issue(t + 2, iN);
+        // ---------- A: own column of t+2; (float rings: the own point's RK base
+        // starts its way into shared memory); plane t+1's box is converted, beside
+        // the inviscid x/y sums of plane t; after the barrier, plane t+2's box
+        // starts its way in (converted at the next plane)
+        // No barrier ends the plane (neb), so a warp that has finished plane t's
+        // update goes on to plane t+1's loads, box wait and conversion while others
+        // still run phase E.  What makes that safe: plane t+2's box goes into the
+        // slot of plane t-1 only after phase A's barrier, which every thread passes
+        // after its phase-E reads of that slot; and what phases E and F read of
+        // plane t's primitive and (mu, p) slots, which the next plane's conversion
+        // overwrites, is read before barrier C.  FP64 stage time 3.5% lower together
+        // with the split own-column conversion below (alone 1% higher); float 1%
+        // lower.  CHAN_END_BAR restores the barrier, for measurement.
+#ifndef CHAN_END_BAR
+        constexpr bool neb = !S::tma_base;
+#else
+        constexpr bool neb = false;
+#endif
+        if (t < ke && !neb) issue(t + 2, iN);
         const bool need_base = P.rk_mode != 0;
         if (S::tma_base && need_base) issue_base(t);
         if (S::prefetch_base) {
@@ -1088,7 +1105,11 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // FP64: plane t+3's own column into L1 a plane before it is loaded (1.8% of the
         // FP64 stage time; the float kernels, which load plane t+2 in phase C, are
         // slower with it)
+#ifndef CHAN_NO_T3_PREFETCH
         if (sizeof(R) == 8 && col_ok && t + 3 <= n3) {
+#else
+        if (false) {
+#endif
             const QI *src = qin() + (long long)(t + 3) * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
@@ -1114,7 +1135,10 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         }
 #endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
-#ifdef CHAN_T2_SPLIT
+        // FP64: plane t+2's own column is loaded before the box wait and converted
+        // after it, in the straight-line block of the box conversion (1.9% of the
+        // stage time alone, 3.5% with neb); CHAN_T2_JOINED converts it at its load
+#ifndef CHAN_T2_JOINED
         constexpr bool t2_split = !late_t2;
 #else
         constexpr bool t2_split = false;
@@ -1164,6 +1188,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         bad = !wait_slot(iP);
         convert(t + 1, iP, pP, mP, true, t2_prims);
         if (__syncthreads_or(bad)) { give_up(); return; }
+        if (t < ke && neb) issue(t + 2, iN);
 
         // ---------- C: viscous flux vectors
         const Slot s0 = slot(pZ), sp = slot(pP);
@@ -1215,6 +1240,17 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
             }
         }
+        // without the end-of-plane barrier, the next plane's conversion overwrites
+        // plane t's primitive and (mu, p) slots while this plane's phase E may still
+        // run: what phases E and F read of them is read here, before barrier C
+        R w0n = R(0), mu0n = R(0), T0n = R(0);
+        if (neb) {
+            um1 = s0.U[bc]; vm1 = s0.V[bc];   // plane t-1's u, v are not read after phase C
+            w0n = s0.W[bc];
+            mu0n = smu(mZ)[bc];
+            if (buoy) T0n = s0.T[bc];
+            keep_halo(s0);
+        }
         if (S::tma_base && need_base) {
             bad = !wait_slot(3);
             if (__syncthreads_or(bad)) { give_up(); return; }
@@ -1250,7 +1286,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
 #endif
             R Fs[5];   // sum of the flux derivatives
-            const R mu0 = smu(mZ)[bc];
+            const R mu0 = neb ? mu0n : smu(mZ)[bc];
             if (xy_a) {
                 // (F1 + G1) from phase A, then the viscous x and y terms
                 Fs[0] = Fxy[0];
@@ -1315,7 +1351,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
             // z
             {
-                const R w0 = s0.W[bc], wp1 = sp.W[bc];
+                const R w0 = neb ? w0n : s0.W[bc], wp1 = sp.W[bc];
                 R w[5];
                 if (t < 3 || t > n3 - 2) {
                     const R c2 = ktab<R>(P, 0, t);
@@ -1367,7 +1403,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 const double tau = P.stat[23 * n3 + 0] - P.stat[23 * n3 + 1];
                 const double rb = P.stat[t - 1];
                 src2 = (0.5 * tau) * rb;
-                src5 = (((P.ggM * (double)s0.U[bc]) * 0.5) * tau) * rb;
+                src5 = (((P.ggM * (double)(neb ? um1 : s0.U[bc])) * 0.5) * tau) * rb;
             }
             double Rd[5];
             Rd[0] = -(double)Fs[0];
@@ -1376,9 +1412,9 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             Rd[3] = -(double)Fs[3];
             if (buoy) {
                 // buoyancy on the wall-normal momentum and its work on the energy
-                const double bq = P.ri * ((double)q0[0] * ((double)s0.T[bc] - P.tref));
+                const double bq = P.ri * ((double)q0[0] * ((double)(neb ? T0n : s0.T[bc]) - P.tref));
                 Rd[3] = bq - (double)Fs[3];
-                src5 = src5 + (P.ggM * (double)s0.W[bc]) * bq;
+                src5 = src5 + (P.ggM * (double)(neb ? w0n : s0.W[bc])) * bq;
             }
             Rd[4] = src5 - (double)Fs[4];
             // RK update in double, on the stage input at its stored precision
@@ -1468,15 +1504,19 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 if (!fin) flag_nonfinite(P.status, i, j, t);
             }
         }
-        // ---------- F: plane t becomes t-1; rotate the rings
+        // ---------- F: plane t becomes t-1; rotate the rings (no barrier: see neb)
 #pragma unroll
         for (int c = 0; c < 5; c++) {
             qm2[c] = qm1[c];
             qm1[c] = q0[c];
         }
         wm2 = wm1;
-        um1 = s0.U[bc]; vm1 = s0.V[bc]; wm1 = s0.W[bc];
-        keep_halo(s0);
+        if (neb) {
+            wm1 = w0n;
+        } else {
+            um1 = s0.U[bc]; vm1 = s0.V[bc]; wm1 = s0.W[bc];
+            keep_halo(s0);
+        }
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             hm1[c] = h0[c];
@@ -1488,7 +1528,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             int x = pZ; pZ = pP; pP = x;
             x = mZ; mZ = mP; mP = x;
         }
-        __syncthreads();
+        if (!neb) __syncthreads();
     }
     if (S::prefetch_base) cp_async_wait<0>();
 }
