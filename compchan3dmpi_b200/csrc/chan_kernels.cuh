@@ -539,8 +539,6 @@ struct StageShape {
     // spills it removes; the float kernels 2-3% faster loading it in phase C)
 #if defined(CHAN_EARLY_T2)
     static constexpr bool late_t2 = false, late_qp2 = false;
-#elif defined(CHAN_T2_SPLIT_F)
-    static constexpr bool late_t2 = false, late_qp2 = true;
 #else
     static constexpr bool late_t2 = sizeof(R) == 4, late_qp2 = sizeof(R) == 8;
 #endif
@@ -1105,11 +1103,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // FP64: plane t+3's own column into L1 a plane before it is loaded (1.8% of the
         // FP64 stage time; the float kernels, which load plane t+2 in phase C, are
         // slower with it)
-#ifndef CHAN_NO_T3_PREFETCH
         if (sizeof(R) == 8 && col_ok && t + 3 <= n3) {
-#else
-        if (false) {
-#endif
             const QI *src = qin() + (long long)(t + 3) * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
