@@ -1137,7 +1137,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #else
         constexpr bool t2_split = false;
 #endif
-        const bool c2 = col_ok && t + 2 < n3;
+        const bool own2 = col_ok && t + 2 < n3;   // plane t+2's own column is an interior one
         double cq[5] = {0, 0, 0, 0, 0};
         // plane t+2's own column: the float kernels prefetch it into L1 here and
         // load and convert it in phase C, where its values start to be used; the
@@ -1149,7 +1149,7 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
                 for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
             }
-        } else if (t2_split && c2) {
+        } else if (t2_split && own2) {
             // interior plane t+2: its own column's Q now, its primitives after the box wait
             const long long off = (long long)(t + 2) * plane + colo;
 #pragma unroll
@@ -1169,13 +1169,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             if (t2_split) {
                 double u, v, w, T;
                 prims_from_q(P, cq, u, v, w, T);
-                up2 = c2 ? (R)u : up2;
-                vp2 = c2 ? (R)v : vp2;
-                wp2 = c2 ? (R)w : wp2;
-                Tp2 = c2 ? (R)T : Tp2;
+                up2 = own2 ? (R)u : up2;
+                vp2 = own2 ? (R)v : vp2;
+                wp2 = own2 ? (R)w : wp2;
+                Tp2 = own2 ? (R)T : Tp2;
                 if (!late_qp2) {
 #pragma unroll
-                    for (int c = 0; c < 5; c++) qp2[c] = c2 ? (R)cq[c] : qp2[c];
+                    for (int c = 0; c < 5; c++) qp2[c] = own2 ? (R)cq[c] : qp2[c];
                 }
             }
         };
