@@ -501,12 +501,18 @@ __device__ __forceinline__ void prims_from_q(const KParams &P, const double q[5]
 // hD at t-1, t, t+1 in registers.
 //
 // The Q box of each plane arrives by one tiled bulk tensor copy (TMA) issued
-// two planes ahead by one thread and completed on an mbarrier, so Q is read
-// from DRAM once per stage with no per-thread load instructions; the halo
-// re-reads of neighbouring CTAs come from L2.  Each staged box point is then
-// converted to primitives once per CTA.  The stage whose input is stored in a
-// wider type than the ring (the first stage of the mixed-precision path, double
+// about two thirds of a plane ahead by one thread and completed on an mbarrier,
+// so Q is read from DRAM once per stage with no per-thread load instructions;
+// the halo re-reads of neighbouring CTAs come from L2.  Each staged box point is
+// then converted to primitives once per CTA.  The stage whose input is stored in
+// a wider type than the ring (the first stage of the mixed-precision path, double
 // in, float rings) loads its boxes with per-thread loads instead.
+//
+// A plane takes two CTA barriers: after the box conversion (with which the
+// inviscid x/y sums of the plane and the next own-column conversion share one
+// straight-line block) and after the viscous fluxes.  None ends the plane, so
+// warps that finish the update early go on into the next plane's loads and
+// conversion while the others complete theirs.
 //
 // Types: QI / QO are the storage types of the stage's input and output state,
 // R the type of the shared rings and of the flux arithmetic.  The plain FP64
@@ -1081,23 +1087,9 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         // the own point's RK base into L1 now; the update reads it at the end of
         // the plane (2.7% of the FP64 stage time against loading it there cold)
         if (!S::prefetch_base && !S::tma_base && P.rk_mode != 0 && out_ok) {
-#ifdef CHAN_PREFETCH_BASE_AHEAD
-            // a plane ahead: plane t+1's base now (plane kb's at the chunk's first plane)
-            if (t == kb) {
-                const double *src0 = P.qbase + (long long)t * plane + colo;
-#pragma unroll
-                for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src0 + c * vol));
-            }
-            const double *src = P.qbase + (long long)(t + 1) * plane + colo;
-            if (t < ke) {
-#pragma unroll
-                for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
-            }
-#else
             const double *src = P.qbase + (long long)t * plane + colo;
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
-#endif
         }
 #endif
         // FP64: plane t+3's own column into L1 a plane before it is loaded (1.8% of the
@@ -1108,26 +1100,6 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
 #pragma unroll
             for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + c * vol));
         }
-#ifdef CHAN_PREFETCH_TABLES
-        // next plane's per-plane coefficients and forcing density into L1 (one lane each)
-        if (t < ke && tid < 6) {
-            const double *a = tid == 0 ? P.czh : (tid == 1 ? P.cz8 : (tid == 2 ? P.cz12 : (tid == 3 ? P.pez : P.stat)));
-            const int k = tid == 4 ? t : (tid == 5 ? t + 2 : t + 1);
-            if (tid != 5 || t + 2 <= n3) asm volatile("prefetch.global.L1 [%0];" ::"l"(tid == 5 ? P.czh + k : a + k));
-        }
-#endif
-#ifdef CHAN_PREFETCH_BOX_L1
-        // per-thread box loads: plane t+2's box into L1 now, converted at the next plane
-        if (!TMA && t + 2 <= n3) {
-#pragma unroll
-            for (int l = 0; l < NL; l++) {
-                if (lp[l] < 0) continue;
-                const QI *src = qin() + (long long)(t + 2) * plane + lo[l];
-#pragma unroll
-                for (int v = 0; v < 5; v++) asm volatile("prefetch.global.L1 [%0];" ::"l"(src + v * vol));
-            }
-        }
-#endif
         R qp2[5] = {0, 0, 0, 0, 0}, up2 = 0, vp2 = 0, wp2 = 0, Tp2 = 0;
         // FP64: plane t+2's own column is loaded before the box wait and converted
         // after it, in the straight-line block of the box conversion (1.9% of the
