@@ -866,14 +866,33 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
     // under a non-periodic wall BC).  hD on a wall plane reads the wall's own
     // values from memory instead (hflux_wall).
     auto no_extra = []() {};
+    // FP64 rings: mu (and p) formed and stored at every box point, not only on R1,
+    // where they are read (the other cells of the slot are never read): the
+    // conversion's block then has no branch on R1, and the 1.31 -> 1.69 powers per
+    // output cost less than the divergent branch did (2.9% of the FP64 stage time;
+    // the float kernels, whose float mu is cheap, are 0.9% slower with it).
+    // CHAN_MU_R1 keeps the branch, for measurement.
+#ifdef CHAN_MU_R1
+    constexpr bool mu_all = false;
+#else
+    constexpr bool mu_all = sizeof(R) == 8;
+#endif
     auto convert = [&](int m, int s, int po, int mo, bool with_xy, auto &&extra) {
         const Slot sl = slot(po);
         R *MU = smu(mo), *PR = sMP + mo + NB;
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
         auto one = [&](int l, bool wall_plane) {
-            if (lp[l] < 0) return;
-            const int p = lp[l] & 0xffff;
+#ifdef CHAN_L0_ALL
+            // staged boxes, interior planes: the first point of every thread (always
+            // inside the box) is converted even where it lies beyond the array (the
+            // copy fills it with zeros; no valid point's stencil reads it)
+            const bool all = TMA && l == 0 && !wall_plane && NT <= NB;
+#else
+            const bool all = false;
+#endif
+            if (!all && lp[l] < 0) return;
+            const int p = all ? tid : (lp[l] & 0xffff);
             const bool r1 = (lp[l] & 0x10000) != 0;
             double q[5];
             if (!TMA) {
@@ -902,13 +921,13 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                 }
                 prims_from_q(P, q, u, vv, w, T);
                 pr = (q[0] * T) * P.inv_gM2;
-                mu = r1 ? mu_of<R>(T) : R(0);
+                mu = mu_all ? mu_of<R>(T) : (r1 ? mu_of<R>(T) : R(0));
             }
             ((R *)sl.U)[p] = (R)u;
             ((R *)sl.V)[p] = (R)vv;
             ((R *)sl.W)[p] = (R)w;
             ((R *)sl.T)[p] = (R)T;
-            if (r1) {
+            if (mu_all || r1) {
                 MU[p] = mu;
                 if (S::p_ring) PR[p] = (R)pr;
             }
