@@ -883,16 +883,8 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
         const bool wall = (m == 1 || m == n3);
         const double *W = P.wp + (size_t)(m == 1 ? 0 : 8) * plane;
         auto one = [&](int l, bool wall_plane) {
-#ifdef CHAN_L0_ALL
-            // staged boxes, interior planes: the first point of every thread (always
-            // inside the box) is converted even where it lies beyond the array (the
-            // copy fills it with zeros; no valid point's stencil reads it)
-            const bool all = TMA && l == 0 && !wall_plane && NT <= NB;
-#else
-            const bool all = false;
-#endif
-            if (!all && lp[l] < 0) return;
-            const int p = all ? tid : (lp[l] & 0xffff);
+            if (lp[l] < 0) return;
+            const int p = lp[l] & 0xffff;
             const bool r1 = (lp[l] & 0x10000) != 0;
             double q[5];
             if (!TMA) {
