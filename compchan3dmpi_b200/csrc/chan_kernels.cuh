@@ -1182,8 +1182,25 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
                     for (int c = 0; c < 5; c++) qp2[c] = (R)q[c];
                     up2 = (R)u; vp2 = (R)v; wp2 = (R)w; Tp2 = (R)T;
                 }
-                if (t + 1 != n3)
+                // FP64 rings: hD(t+1) on every plane (on the top wall plane it reads the
+                // wall's valid ring values and is not used), so that it shares one
+                // straight-line block with fD and gD (0.9% of the FP64 stage time; the
+                // float kernels keep the uniform branch, 0.2% faster).  CHAN_HFLUX_GUARD
+                // keeps the branch in the FP64 kernel too, for measurement.
+#ifdef CHAN_HFLUX_GUARD
+                constexpr bool hflux_all = false;
+#else
+                constexpr bool hflux_all = sizeof(R) == 8;
+#endif
+                if (hflux_all) {
+                    R h[4];
+                    hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, h);
+                    const bool hok = t + 1 != n3;
+#pragma unroll
+                    for (int c = 0; c < 4; c++) hp1[c] = hok ? h[c] : R(0);
+                } else if (t + 1 != n3) {
                     hflux(t + 1, pP, mP, iP, s0.U[bc], s0.V[bc], s0.W[bc], s0.T[bc], up2, vp2, wp2, Tp2, hp1);
+                }
                 R g[4];
                 visc_fxy<BX, R, S::p_ring>(C, s0, um1, vm1, wm1, sp, MU, PR, bc, czt, fown, g);
 #pragma unroll
