@@ -1347,7 +1347,30 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             {
                 const R w0 = neb ? w0n : s0.W[bc], wp1 = sp.W[bc];
                 R w[5];
-                if (t < 3 || t > n3 - 2) {
+                // FP64 rings: the second-order weights of the planes next to the walls
+                // and the hybrid ones both formed and selected by the (uniform) plane
+                // test, so that the update's block has no branch (0.7% of the FP64 stage
+                // time); CHAN_ZW_BRANCH keeps the branch, for measurement
+#ifdef CHAN_ZW_BRANCH
+                constexpr bool zw_sel = false;
+#else
+                constexpr bool zw_sel = sizeof(R) == 8;
+#endif
+                if (zw_sel) {
+                    // both weight sets, selected by the (uniform) plane test: no branch
+                    // in the update's block (the tables hold nP3+2 entries, so the
+                    // interior set's reads stay in range on every plane)
+                    const bool near = t < 3 || t > n3 - 2;
+                    const R c2 = ktab<R>(P, 0, t);
+                    const bool qk = (ktab<R>(P, 3, t) * fabs(q0[3])) > C.pez_val * mu0;
+                    R wi[5];
+                    inv_weights(wm2, wm1, w0, wp1, wp2, qk, ktab<R>(P, 1, t), ktab<R>(P, 2, t), wi);
+                    w[0] = near ? R(0) : wi[0];
+                    w[1] = near ? -(wm1 * c2) : wi[1];
+                    w[2] = near ? R(0) : wi[2];
+                    w[3] = near ? wp1 * c2 : wi[3];
+                    w[4] = near ? R(0) : wi[4];
+                } else if (t < 3 || t > n3 - 2) {
                     const R c2 = ktab<R>(P, 0, t);
                     w[0] = R(0); w[1] = -(wm1 * c2); w[2] = R(0); w[3] = wp1 * c2; w[4] = R(0);
                 } else {
