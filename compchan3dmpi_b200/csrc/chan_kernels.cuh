@@ -1416,7 +1416,25 @@ __device__ __forceinline__ void stage_body(const KParams &P, const CUtensorMap *
             }
             // source: lagged wall-shear forcing (main_v1.9.f90:565-571), in double
             double src2 = 0.0, src5 = 0.0;
-            if (P.force_on) {
+            // FP64 rings: the forcing terms formed on every launch (the statistics
+            // array always holds these entries) and selected by the flag, so that the
+            // update's block has no branch on it (1.1% of the FP64 stage time);
+            // CHAN_FORCE_BRANCH keeps the branch, for measurement
+#if defined(CHAN_FORCE_BRANCH)
+            constexpr bool force_sel = false;
+#elif defined(CHAN_FORCE_SEL_F)
+            constexpr bool force_sel = true;
+#else
+            constexpr bool force_sel = sizeof(R) == 8;
+#endif
+            if (force_sel) {
+                const double tau = P.stat[23 * n3 + 0] - P.stat[23 * n3 + 1];
+                const double rb = P.stat[t - 1];
+                const double s2 = (0.5 * tau) * rb;
+                const double s5 = (((P.ggM * (double)(neb ? um1 : s0.U[bc])) * 0.5) * tau) * rb;
+                src2 = P.force_on ? s2 : 0.0;
+                src5 = P.force_on ? s5 : 0.0;
+            } else if (P.force_on) {
                 const double tau = P.stat[23 * n3 + 0] - P.stat[23 * n3 + 1];
                 const double rb = P.stat[t - 1];
                 src2 = (0.5 * tau) * rb;
